@@ -1,0 +1,241 @@
+"""ctypes binding of the C ABI in include/hisv.h (libhisv.so).
+
+This is the thin Python view of the drop-in boundary used by the tests, the
+benchmark and the Python-level helpers; the pybind11 module
+``svsimulator_py_wrapper`` binds the same library with the reference's class
+names.  There is no CPU fallback: if libhisv.so is missing, or a call needs a
+GPU and none is visible, an error is raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .gates import HS_GATE_DTYPE, Gate, to_records
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhisv.so")
+
+HS_OK = 0
+HS_E_INVALID = -1
+HS_E_NOMEM = -2
+HS_E_CUDA = -3
+HS_E_UNSUPPORTED = -4
+HS_E_TIMEOUT = -5
+HS_E_NODEVICE = -6
+C128 = 0
+C64 = 1
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_u64 = ctypes.c_uint64
+_u32 = ctypes.c_uint32
+_dp = ctypes.POINTER(ctypes.c_double)
+_llp = ctypes.POINTER(ctypes.c_longlong)
+
+# name -> argtypes (all return int unless listed in _RESTYPE)
+SIGNATURES = {
+    "hs_last_error": [],
+    "hs_version": [],
+    "hs_device_count": [ctypes.POINTER(_i)],
+    "hs_state_create": [_i, _i, ctypes.POINTER(_vp)],
+    "hs_state_destroy": [_vp],
+    "hs_state_num_qubits": [_vp, ctypes.POINTER(_i)],
+    "hs_state_dtype": [_vp, ctypes.POINTER(_i)],
+    "hs_state_device_ptr": [_vp, ctypes.POINTER(_vp)],
+    "hs_state_qubit_to_slot": [_vp, _vp],
+    "hs_state_set_basis": [_vp, _u64, _vp],
+    "hs_state_copy_to_host": [_vp, _vp, _u64, _u64, _vp],
+    "hs_state_copy_from_host": [_vp, _vp, _u64, _u64, _vp],
+    "hs_state_canonicalize": [_vp, _vp],
+    "hs_state_convert": [_vp, _vp, _vp],
+    "hs_gate_apply": [_vp, _vp, _vp],
+    "hs_part_run": [_vp, _vp, _i, _vp],
+    "hs_parts_run": [_vp, _vp, _vp, _i, _vp],
+    "hs_set_tile_qubits": [_i],
+    "hs_permute_bits": [_vp, _vp, _i, _vp],
+    "hs_gather_qubits": [_vp, _vp, _i, _vp],
+    "hs_norm2": [_vp, _dp],
+    "hs_inner": [_vp, _vp, _dp],
+    "hs_max_abs_diff": [_vp, _vp, _dp],
+    "hs_probability": [_vp, _i, _i, _dp],
+    "hs_expect_zz": [_vp, _vp, _i, _dp],
+    "hs_measure": [_vp, _vp, _i, _u32, _u64, _vp],
+    "hs_counters": [_llp, _llp, _llp],
+    "hs_counters_reset": [],
+    "hs_set_timing": [_i],
+}
+_RESTYPE = {"hs_last_error": ctypes.c_char_p}
+
+
+class HisvError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hisv error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libhisv.so once (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built: run `python -m hisvsim_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RESTYPE.get(name, ctypes.c_int)
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != HS_OK:
+        raise HisvError(rc, lib().hs_last_error().decode(errors="replace"))
+    return rc
+
+
+def device_count() -> int:
+    c = _i(0)
+    check(lib().hs_device_count(ctypes.byref(c)))
+    return c.value
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _records(gates) -> np.ndarray:
+    if isinstance(gates, np.ndarray) and gates.dtype == HS_GATE_DTYPE:
+        return np.ascontiguousarray(gates)
+    return to_records(list(gates))
+
+
+class State:
+    """A device-resident state vector (hs_state)."""
+
+    def __init__(self, n: int, dtype: int = C128):
+        h = _vp()
+        check(lib().hs_state_create(n, dtype, ctypes.byref(h)))
+        self.h = h
+        self.n = n
+        self.dtype = dtype
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hs_state_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def np_dtype(self):
+        return np.complex128 if self.dtype == C128 else np.complex64
+
+    def set_basis(self, x: int, stream=None):
+        check(lib().hs_state_set_basis(self.h, x, stream))
+
+    def qubit_to_slot(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.int32)
+        check(lib().hs_state_qubit_to_slot(self.h, _ptr(out)))
+        return out
+
+    def raw(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        """Slot-ordered amplitudes [first, first+count)."""
+        count = (1 << self.n) - first if count is None else count
+        out = np.empty(count, dtype=self.np_dtype)
+        check(lib().hs_state_copy_to_host(self.h, _ptr(out), first, count, None))
+        return out
+
+    def load(self, amps: np.ndarray, first: int = 0):
+        a = np.ascontiguousarray(amps, dtype=self.np_dtype)
+        check(lib().hs_state_copy_from_host(self.h, _ptr(a), first, a.size, None))
+
+    def canonicalize(self, stream=None):
+        check(lib().hs_state_canonicalize(self.h, stream))
+
+    def amplitudes(self) -> np.ndarray:
+        """Amplitudes in qubit order (canonicalizes the slot map first)."""
+        self.canonicalize()
+        return self.raw()
+
+    def apply(self, gate, stream=None):
+        rec = _records([gate] if isinstance(gate, Gate) else gate)
+        check(lib().hs_gate_apply(self.h, _ptr(rec), stream))
+
+    def run_part(self, gates, stream=None):
+        rec = _records(gates)
+        check(lib().hs_part_run(self.h, _ptr(rec), len(rec), stream))
+
+    def run_parts(self, records: np.ndarray, offsets: np.ndarray, stream=None):
+        records = _records(records)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        check(lib().hs_parts_run(self.h, _ptr(records), _ptr(offsets), len(offsets) - 1, stream))
+
+    def permute_bits(self, pairs: Sequence[int], stream=None):
+        p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1)
+        check(lib().hs_permute_bits(self.h, _ptr(p), len(p) // 2, stream))
+
+    def gather_qubits(self, proc_qubits: Sequence[int], stream=None):
+        p = np.ascontiguousarray(proc_qubits, dtype=np.int32)
+        check(lib().hs_gather_qubits(self.h, _ptr(p), len(p), stream))
+
+    def norm2(self) -> float:
+        out = ctypes.c_double()
+        check(lib().hs_norm2(self.h, ctypes.byref(out)))
+        return out.value
+
+    def inner(self, other: "State") -> complex:
+        out = (ctypes.c_double * 2)()
+        check(lib().hs_inner(self.h, other.h, out))
+        return complex(out[0], out[1])
+
+    def max_abs_diff(self, other: "State") -> float:
+        out = ctypes.c_double()
+        check(lib().hs_max_abs_diff(self.h, other.h, ctypes.byref(out)))
+        return out.value
+
+    def probability(self, qubit: int, value: int = 0) -> float:
+        out = ctypes.c_double()
+        check(lib().hs_probability(self.h, qubit, value, ctypes.byref(out)))
+        return out.value
+
+    def expect_zz(self, pairs) -> np.ndarray:
+        p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1)
+        out = np.zeros(len(p) // 2)
+        check(lib().hs_expect_zz(self.h, _ptr(p), len(p) // 2,
+                                 out.ctypes.data_as(_dp)))
+        return out
+
+    def measure(self, qubits: Sequence[int], nsamples: int, seed: int) -> np.ndarray:
+        q = np.ascontiguousarray(qubits, dtype=np.int32)
+        out = np.zeros((nsamples, len(q)), dtype=np.int32)
+        check(lib().hs_measure(self.h, _ptr(q), len(q), nsamples, seed, _ptr(out)))
+        return out
+
+
+def set_tile_qubits(m: int) -> int:
+    rc = lib().hs_set_tile_qubits(m)
+    if rc < 0:
+        check(rc)
+    return rc
+
+
+def counters():
+    a, g, p = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    check(lib().hs_counters(ctypes.byref(a), ctypes.byref(g), ctypes.byref(p)))
+    return {"apply_us": a.value, "gates": g.value, "passes": p.value}
+
+
+def counters_reset():
+    check(lib().hs_counters_reset())

@@ -1,0 +1,159 @@
+// Internal declarations shared by the host code and the kernels of libhisv.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "hisv.h"
+
+namespace hisv {
+
+using cplx = std::complex<double>;
+
+// ---- errors ---------------------------------------------------------------
+int set_error(int code, const char* fmt, ...);
+#define HS_CUDA(call)                                                              \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return ::hisv::set_error(HS_E_CUDA, "%s: %s (%s:%d)", #call,                 \
+                               cudaGetErrorString(e_), __FILE__, __LINE__);        \
+  } while (0)
+#define HS_TRY(expr)            \
+  do {                          \
+    int rc_ = (expr);           \
+    if (rc_ != HS_OK) return rc_; \
+  } while (0)
+
+// ---- gate lowering (gatemath.cpp) ------------------------------------------
+// A gate lowered to its matrix on 1 or 2 targets, in the reference's index
+// convention: for 2 targets, local index i = 2*b(target0) + b(target1)
+// (basic_gates.hpp:992-1004).  Controls are kept as qubits.
+struct LoweredGate {
+  int nt = 1;                 // 0 = identity (dropped), 1 or 2
+  int targets[2] = {0, 0};    // qubits
+  int nc = 0;
+  int controls[HS_MAX_CONTROLS] = {0, 0, 0, 0, 0};
+  cplx m[16];                 // row-major 2x2 or 4x4
+};
+// Returns HS_OK or HS_E_INVALID (message set) for gates the reference rejects.
+int lower_gate(const hs_gate& g, int num_qubits, LoweredGate* out);
+
+// ---- K1 part program --------------------------------------------------------
+constexpr int kRegBits = 4;        // amplitudes per thread = 2^kRegBits
+constexpr int kMaxTileBits = 13;   // 2^13 complex128 = 128 KiB of shared memory
+constexpr int kMaxOps = 160;
+constexpr int kMaxCoef = 640;      // complex coefficients (double2)
+constexpr int kMaxGroups = 48;
+constexpr int kMaxRuns = 16;
+
+enum OpKind : uint8_t {
+  OP1_DENSE = 0,  // 2x2
+  OP1_DIAG = 1,   // diag(d0, d1)
+  OP1_PHASE = 2,  // diag(1, d1)
+  OP1_NEG = 3,    // diag(1, -1)
+  OP1_X = 4,      // [[0,1],[1,0]]
+  OP1_H = 5,      // s*[[1,1],[1,-1]], s = 1/sqrt(2)
+  OP1_Y = 6,      // [[0,-i],[i,0]]
+  OP2_DENSE = 8,  // 4x4
+  OP2_DIAG = 9,   // diag(4)
+  OP2_SWAP = 10,  // swap |01>,|10>
+};
+
+struct DevOp {
+  uint8_t kind;
+  uint8_t ja, jb;     // register-bit positions of the targets (ja < jb for 2q)
+  uint8_t pad;
+  uint16_t coef;      // first coefficient (index into PartProgram::coef)
+  uint16_t creg;      // controls that are register bits, in register-element space
+  uint32_t cthr;      // controls that are thread bits, in tile-index space
+  uint32_t pad2;
+  uint64_t couter;    // controls outside the tile, in global-index space
+};
+static_assert(sizeof(DevOp) == 24, "DevOp layout");
+
+struct Runs {  // bit-run deposit: out |= ((x >> src) & (2^len - 1)) << dst
+  uint8_t n;
+  uint8_t src[kMaxRuns];
+  uint8_t len[kMaxRuns];
+  uint8_t dst[kMaxRuns];
+};
+
+struct GroupDesc {
+  uint8_t reg_tbit[kRegBits];  // tile bit held by register bit j
+  uint16_t first_op, num_ops;
+  Runs thr;                    // thread index -> tile index
+};
+
+struct PartProgram {
+  int32_t n;           // qubits (slots) of the state
+  int32_t m;           // tile bits
+  int32_t ngroups;
+  int32_t nops;
+  int32_t ncoef;
+  int32_t pad;
+  uint64_t ntiles;     // 2^(n-m)
+  Runs tile;           // tile index -> global index
+  Runs outer;          // tile number -> global index
+  GroupDesc groups[kMaxGroups];
+  DevOp ops[kMaxOps];
+  double2 coef[kMaxCoef];
+};
+static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
+
+// Build the K1 programs for a sequence of lowered gates on a state whose
+// qubit q sits in slot q2s[q].  Long parts produce several programs (each one
+// state pass).  Returns HS_OK or an error.
+int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
+              int tile_bits_hint, std::vector<PartProgram>* programs);
+
+// ---- K2 bit-swap program ----------------------------------------------------
+struct PermProgram {
+  int32_t n;
+  int32_t m;            // tile bits (low run + low-high partners)
+  uint64_t ntiles;      // tiles of the tile space (before orbit pairing)
+  Runs tile;            // tile index -> global index (source layout)
+  Runs outer;           // tile number -> global index
+  uint32_t tile_swap_src;   // in tile-index space: bit pairs swapped inside a tile
+  uint8_t ntswap;
+  uint8_t tsa[32], tsb[32]; // tile-bit pairs swapped inside the tile
+  uint64_t hh_mask_a, hh_mask_b;  // disjoint high-high pairs (global bits)
+  uint8_t nhh;
+  uint8_t hha[32], hhb[32];
+};
+
+// ---- launchers (kernels_*.cu) ----------------------------------------------
+int launch_part(void* amp, int dtype, const PartProgram& prog, cudaStream_t s);
+int launch_permute(void* amp, int dtype, int n, const int32_t* pairs, int npairs,
+                   cudaStream_t s);
+int reduce_norm2(const void* amp, int dtype, int n, double* out, cudaStream_t s);
+int reduce_inner(const void* a, const void* b, int dtype, int n, double out[2],
+                 cudaStream_t s);
+int reduce_maxdiff(const void* a, const void* b, int dtype, int n, double* out,
+                   cudaStream_t s);
+int reduce_prob0(const void* amp, int dtype, int n, int slot, double* out, cudaStream_t s);
+int reduce_zz(const void* amp, int dtype, int n, const int32_t* slot_pairs, int npairs,
+              double* out, cudaStream_t s);
+int reduce_chunks(const void* amp, int dtype, int n, int chunk_bits, double* host_out,
+                  cudaStream_t s);
+int set_basis_kernel(void* amp, int dtype, int n, uint64_t index, cudaStream_t s);
+int convert_kernel(const void* src, int sdtype, void* dst, int ddtype, uint64_t count,
+                   cudaStream_t s);
+
+// ---- counters ---------------------------------------------------------------
+void count_pass(long long gates);
+
+inline size_t amp_bytes(int dtype) { return dtype == HS_DTYPE_C64 ? 8 : 16; }
+
+}  // namespace hisv
+
+struct hs_state {
+  int n = 0;
+  int dtype = HS_DTYPE_C128;
+  void* amp = nullptr;  // device, slot-ordered
+  std::vector<int> q2s, s2q;
+};

@@ -1,0 +1,343 @@
+// K2 (in-place bit-swap permutation), K3 (FP64 reductions) and small
+// elementwise kernels (basis-state set, dtype conversion).
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+
+namespace hisv {
+namespace {
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// ---- K2 -------------------------------------------------------------------
+// Replaces the MPI redistribution (gather_slots, mpi_redistributer.hpp:265-344)
+// on one device.  A set of disjoint slot-bit pairs (a_i, b_i) defines the
+// involution P(x) = x with bits a_i and b_i exchanged; amplitude x moves to
+// P(x).  Because P is an involution the pass is in place: the thread that owns
+// x < P(x) swaps the two amplitudes; fixed points are skipped.
+struct SwapPairs {
+  int np;
+  uint64_t ma, mb;  // masks of the a and b bits
+  uint8_t a[32], b[32];
+};
+
+template <typename V>
+__global__ void __launch_bounds__(256) k2_bitswap(V* __restrict__ sv, uint64_t size,
+                                                  const SwapPairs sp) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t x = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; x < size; x += stride) {
+    // pairs whose two bits differ in x flip; others are unchanged
+    uint64_t y = x;
+#pragma unroll 4
+    for (int i = 0; i < sp.np; ++i) {
+      const uint64_t ba = (x >> sp.a[i]) & 1ull, bb = (x >> sp.b[i]) & 1ull;
+      y ^= (ba ^ bb) * ((1ull << sp.a[i]) | (1ull << sp.b[i]));
+    }
+    if (x < y) {
+      V u = sv[x], w = sv[y];
+      sv[x] = w;
+      sv[y] = u;
+    }
+  }
+}
+
+// ---- K3 ---------------------------------------------------------------------
+// Deterministic two-stage sums in FP64: a fixed grid, a fixed per-thread
+// stride, a fixed tree inside each block, then one block adds the per-block
+// partials in order.  (The reference's probability() accumulates into one
+// variable from all OpenMP threads, state_vector.hpp:908-914, which races.)
+constexpr int kRedBlocks = 1184;  // 8 x 148
+constexpr int kRedThreads = 256;
+
+template <typename V>
+__device__ __forceinline__ double2 ld2(const V* p, uint64_t i) {
+  V v = p[i];
+  return make_double2(double(v.x), double(v.y));
+}
+
+__device__ __forceinline__ double block_sum(double x, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = x;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < int(blockDim.x >> 5); ++i) r += sh[i];
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ double block_max(double x, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = x;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < int(blockDim.x >> 5); ++i) r = fmax(r, sh[i]);
+  __syncthreads();
+  return r;
+}
+
+enum RedKind { RED_NORM = 0, RED_PROB0 = 1, RED_ZZ = 2, RED_INNER = 3, RED_MAXDIFF = 4 };
+
+// partial[k * gridDim.x + blockIdx.x] for k < nout
+template <typename V>
+__global__ void __launch_bounds__(kRedThreads) k3_reduce(const V* __restrict__ a,
+                                                         const V* __restrict__ b, uint64_t size,
+                                                         int kind, uint64_t m1, uint64_t m2,
+                                                         double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  double s0 = 0, s1 = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < size; i += stride) {
+    const double2 u = ld2(a, i);
+    if (kind == RED_NORM) {
+      s0 += u.x * u.x + u.y * u.y;
+    } else if (kind == RED_PROB0) {
+      if (!(i & m1)) s0 += u.x * u.x + u.y * u.y;
+    } else if (kind == RED_ZZ) {
+      const double p = u.x * u.x + u.y * u.y;
+      const bool odd = (__popcll(i & m1) + __popcll(i & m2)) & 1;
+      s0 += odd ? -p : p;
+    } else if (kind == RED_INNER) {
+      const double2 w = ld2(b, i);  // conj(u) * w
+      s0 += u.x * w.x + u.y * w.y;
+      s1 += u.x * w.y - u.y * w.x;
+    } else {
+      const double2 w = ld2(b, i);
+      const double dx = u.x - w.x, dy = u.y - w.y;
+      s0 = fmax(s0, sqrt(dx * dx + dy * dy));
+    }
+  }
+  if (kind == RED_MAXDIFF) {
+    const double r = block_max(s0, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = r;
+  } else {
+    const double r0 = block_sum(s0, sh);
+    const double r1 = block_sum(s1, sh);
+    if (threadIdx.x == 0) {
+      partial[blockIdx.x] = r0;
+      partial[gridDim.x + blockIdx.x] = r1;
+    }
+  }
+}
+
+__global__ void k3_finish(const double* __restrict__ partial, int nblocks, int kind,
+                          double* __restrict__ out) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int k = 0; k < 2; ++k) {
+    double s = kind == RED_MAXDIFF ? 0.0 : 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+      const double v = partial[k * nblocks + i];
+      s = kind == RED_MAXDIFF ? fmax(s, v) : s + v;
+    }
+    const double r = kind == RED_MAXDIFF ? block_max(s, sh) : block_sum(s, sh);
+    if (threadIdx.x == 0) out[k] = r;
+    if (kind == RED_MAXDIFF) break;
+  }
+}
+
+template <typename V>
+int run_reduce(const void* a, const void* b, int n, int kind, uint64_t m1, uint64_t m2,
+               double out[2], cudaStream_t s) {
+  const uint64_t size = 1ull << n;
+  const int blocks = int(std::min<uint64_t>(kRedBlocks, (size + kRedThreads - 1) / kRedThreads));
+  double* scratch = nullptr;  // [2*blocks partials | 2 results]
+  HS_CUDA(cudaMallocAsync(&scratch, sizeof(double) * (2 * blocks + 2), s));
+  k3_reduce<V><<<blocks, kRedThreads, 0, s>>>(static_cast<const V*>(a),
+                                               static_cast<const V*>(b), size, kind, m1, m2,
+                                               scratch);
+  k3_finish<<<1, kRedThreads, 0, s>>>(scratch, blocks, kind, scratch + 2 * blocks);
+  cudaError_t e1 = cudaGetLastError();
+  double host[2] = {0, 0};
+  cudaError_t e2 = cudaMemcpyAsync(host, scratch + 2 * blocks, sizeof(host),
+                                   cudaMemcpyDeviceToHost, s);
+  cudaError_t e3 = cudaFreeAsync(scratch, s);
+  cudaError_t e4 = cudaStreamSynchronize(s);
+  for (cudaError_t e : {e1, e2, e3, e4})
+    if (e != cudaSuccess)
+      return set_error(HS_E_CUDA, "reduction: %s", cudaGetErrorString(e));
+  out[0] = host[0];
+  out[1] = host[1];
+  return HS_OK;
+}
+
+int reduce_any(const void* a, const void* b, int dtype, int n, int kind, uint64_t m1,
+               uint64_t m2, double out[2], cudaStream_t s) {
+  if (dtype == HS_DTYPE_C128) return run_reduce<double2>(a, b, n, kind, m1, m2, out, s);
+  return run_reduce<float2>(a, b, n, kind, m1, m2, out, s);
+}
+
+// per-chunk probability mass: block b sums |a_i|^2 over chunk b (fixed order)
+template <typename V>
+__global__ void __launch_bounds__(kRedThreads) k3_chunks(const V* __restrict__ a, int chunk_bits,
+                                                         double* __restrict__ out) {
+  __shared__ double sh[kRedThreads / 32];
+  const uint64_t base = uint64_t(blockIdx.x) << chunk_bits;
+  const uint64_t len = 1ull << chunk_bits;
+  double s = 0;
+  for (uint64_t i = threadIdx.x; i < len; i += blockDim.x) {
+    const double2 u = ld2(a, base + i);
+    s += u.x * u.x + u.y * u.y;
+  }
+  const double r = block_sum(s, sh);
+  if (threadIdx.x == 0) out[blockIdx.x] = r;
+}
+
+template <typename V>
+__global__ void k_set_basis(V* __restrict__ sv, uint64_t size, uint64_t index) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < size; i += stride) {
+    V v;
+    v.x = i == index ? 1 : 0;
+    v.y = 0;
+    sv[i] = v;
+  }
+}
+
+template <typename A, typename B>
+__global__ void k_convert(const A* __restrict__ src, B* __restrict__ dst, uint64_t count) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+    A a = src[i];
+    B b;
+    b.x = decltype(b.x)(a.x);
+    b.y = decltype(b.y)(a.y);
+    dst[i] = b;
+  }
+}
+
+int grid_for(uint64_t size, int threads) {
+  const uint64_t want = uint64_t(num_sms()) * 8;
+  const uint64_t need = (size + threads - 1) / threads;
+  return int(std::max<uint64_t>(1, std::min(want, need)));
+}
+
+}  // namespace
+
+int reduce_chunks(const void* amp, int dtype, int n, int chunk_bits, double* host_out,
+                  cudaStream_t s) {
+  const uint64_t nchunks = 1ull << (n - chunk_bits);
+  double* scratch = nullptr;
+  HS_CUDA(cudaMallocAsync(&scratch, sizeof(double) * nchunks, s));
+  if (dtype == HS_DTYPE_C128)
+    k3_chunks<double2><<<unsigned(nchunks), kRedThreads, 0, s>>>(
+        static_cast<const double2*>(amp), chunk_bits, scratch);
+  else
+    k3_chunks<float2><<<unsigned(nchunks), kRedThreads, 0, s>>>(
+        static_cast<const float2*>(amp), chunk_bits, scratch);
+  cudaError_t e1 = cudaGetLastError();
+  cudaError_t e2 = cudaMemcpyAsync(host_out, scratch, sizeof(double) * nchunks,
+                                   cudaMemcpyDeviceToHost, s);
+  cudaError_t e3 = cudaFreeAsync(scratch, s);
+  cudaError_t e4 = cudaStreamSynchronize(s);
+  for (cudaError_t e : {e1, e2, e3, e4})
+    if (e != cudaSuccess) return set_error(HS_E_CUDA, "chunk sums: %s", cudaGetErrorString(e));
+  return HS_OK;
+}
+
+int launch_permute(void* amp, int dtype, int n, const int32_t* pairs, int npairs,
+                   cudaStream_t s) {
+  if (npairs <= 0) return HS_OK;
+  if (npairs > 32) return set_error(HS_E_INVALID, "at most 32 bit pairs per pass");
+  SwapPairs sp{};
+  sp.np = npairs;
+  for (int i = 0; i < npairs; ++i) {
+    sp.a[i] = uint8_t(pairs[2 * i]);
+    sp.b[i] = uint8_t(pairs[2 * i + 1]);
+    sp.ma |= 1ull << sp.a[i];
+    sp.mb |= 1ull << sp.b[i];
+  }
+  const uint64_t size = 1ull << n;
+  const int threads = 256;
+  if (dtype == HS_DTYPE_C128)
+    k2_bitswap<double2><<<grid_for(size, threads), threads, 0, s>>>(static_cast<double2*>(amp),
+                                                                     size, sp);
+  else
+    k2_bitswap<float2><<<grid_for(size, threads), threads, 0, s>>>(static_cast<float2*>(amp),
+                                                                    size, sp);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
+int reduce_norm2(const void* amp, int dtype, int n, double* out, cudaStream_t s) {
+  double r[2];
+  HS_TRY(reduce_any(amp, amp, dtype, n, RED_NORM, 0, 0, r, s));
+  *out = r[0];
+  return HS_OK;
+}
+
+int reduce_inner(const void* a, const void* b, int dtype, int n, double out[2],
+                 cudaStream_t s) {
+  return reduce_any(a, b, dtype, n, RED_INNER, 0, 0, out, s);
+}
+
+int reduce_maxdiff(const void* a, const void* b, int dtype, int n, double* out,
+                   cudaStream_t s) {
+  double r[2];
+  HS_TRY(reduce_any(a, b, dtype, n, RED_MAXDIFF, 0, 0, r, s));
+  *out = r[0];
+  return HS_OK;
+}
+
+int reduce_prob0(const void* amp, int dtype, int n, int slot, double* out, cudaStream_t s) {
+  double r[2];
+  HS_TRY(reduce_any(amp, amp, dtype, n, RED_PROB0, 1ull << slot, 0, r, s));
+  *out = r[0];
+  return HS_OK;
+}
+
+int reduce_zz(const void* amp, int dtype, int n, const int32_t* slot_pairs, int npairs,
+              double* out, cudaStream_t s) {
+  for (int i = 0; i < npairs; ++i) {
+    double r[2];
+    HS_TRY(reduce_any(amp, amp, dtype, n, RED_ZZ, 1ull << slot_pairs[2 * i],
+                      1ull << slot_pairs[2 * i + 1], r, s));
+    out[i] = r[0];
+  }
+  return HS_OK;
+}
+
+int set_basis_kernel(void* amp, int dtype, int n, uint64_t index, cudaStream_t s) {
+  const uint64_t size = 1ull << n;
+  if (dtype == HS_DTYPE_C128)
+    k_set_basis<double2><<<grid_for(size, 256), 256, 0, s>>>(static_cast<double2*>(amp), size,
+                                                             index);
+  else
+    k_set_basis<float2><<<grid_for(size, 256), 256, 0, s>>>(static_cast<float2*>(amp), size,
+                                                            index);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
+int convert_kernel(const void* src, int sdtype, void* dst, int ddtype, uint64_t count,
+                   cudaStream_t s) {
+  const int g = grid_for(count, 256);
+  if (sdtype == HS_DTYPE_C128 && ddtype == HS_DTYPE_C64)
+    k_convert<double2, float2><<<g, 256, 0, s>>>(static_cast<const double2*>(src),
+                                                 static_cast<float2*>(dst), count);
+  else if (sdtype == HS_DTYPE_C64 && ddtype == HS_DTYPE_C128)
+    k_convert<float2, double2><<<g, 256, 0, s>>>(static_cast<const float2*>(src),
+                                                 static_cast<double2*>(dst), count);
+  else if (sdtype == HS_DTYPE_C128)
+    k_convert<double2, double2><<<g, 256, 0, s>>>(static_cast<const double2*>(src),
+                                                  static_cast<double2*>(dst), count);
+  else
+    k_convert<float2, float2><<<g, 256, 0, s>>>(static_cast<const float2*>(src),
+                                                static_cast<float2*>(dst), count);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
+}  // namespace hisv

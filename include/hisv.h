@@ -1,0 +1,206 @@
+/*
+ * hisv.h — C ABI of the B200-native hierarchical state-vector simulator.
+ *
+ * This is the drop-in boundary for the hot path of pnnl/hisvsim: the per-part
+ * gather -> apply -> scatter update of a state vector (execute.hpp,
+ * state_vector.hpp, loop.hpp, basic_gates.hpp) and the qubit redistribution
+ * (svsim-mpi.hpp, mpi_redistributer.hpp).  The reference exposes that path to
+ * Python through the pybind11 module `svsimulator_py_wrapper`
+ * (py_wrapper.cpp:15-177); the pybind11 module shipped in hisvsim_b200/ binds
+ * the same names onto the functions declared here.  Every entry point below
+ * names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, fixed-width integers, doubles.  A
+ *    CUDA stream is passed as `void*` (NULL = the library's own stream).
+ *  - Every call returns HS_OK (0) or a negative HS_E* code and never aborts;
+ *    hs_last_error() gives a one-line message for the calling thread.
+ *    (The reference asserts / calls exit(); types.hpp:34-37,
+ *    state_vector.hpp:194-196.)
+ *  - Amplitudes are stored slot-ordered, interleaved (re, im): complex128
+ *    (16 B) for HS_DTYPE_C128 and complex64 (8 B) for HS_DTYPE_C64.
+ *  - Qubit q lives in slot qubit_to_slot[q]; amplitude index bit s is slot s
+ *    (state_vector.hpp:41-119 keeps the same qubit<->slot permutation).
+ *  - Calls are stream-ordered; functions that return host values synchronise.
+ */
+#ifndef HISV_H_
+#define HISV_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define HS_OK 0
+#define HS_E_INVALID (-1)     /* bad argument (qubit index, size, type ...) */
+#define HS_E_NOMEM (-2)       /* device or host allocation failed          */
+#define HS_E_CUDA (-3)        /* a CUDA runtime call failed                */
+#define HS_E_UNSUPPORTED (-4) /* valid request outside what is built       */
+#define HS_E_TIMEOUT (-5)     /* a bounded device-side wait expired        */
+#define HS_E_NODEVICE (-6)    /* no CUDA device visible                     */
+
+/* ---- amplitude types ----------------------------------------------------- */
+#define HS_DTYPE_C128 0 /* std::complex<double>, the reference's Type (types.hpp:27) */
+#define HS_DTYPE_C64 1  /* complex64, the precision form                           */
+
+/* ---- gate types: same numbering as SvSim::GateType (basic_gates.hpp:12-44) */
+enum hs_gate_type {
+  HS_GATE_INVALID = 0,
+  HS_GATE_ALLOC = 1,
+  HS_GATE_FREE = 2,
+  HS_GATE_I = 3,
+  HS_GATE_X = 4,
+  HS_GATE_Y = 5,
+  HS_GATE_Z = 6,
+  HS_GATE_H = 7,
+  HS_GATE_S = 8,
+  HS_GATE_T = 9,
+  HS_GATE_RX = 10,
+  HS_GATE_RY = 11,
+  HS_GATE_RZ = 12,
+  HS_GATE_RI = 13,
+  HS_GATE_R1 = 14,
+  HS_GATE_RXFRAC = 15,
+  HS_GATE_RYFRAC = 16,
+  HS_GATE_RZFRAC = 17,
+  HS_GATE_RIFRAC = 18,
+  HS_GATE_R1FRAC = 19,
+  HS_GATE_SWAP = 20,
+  HS_GATE_C1 = 21,
+  HS_GATE_C2 = 22,
+  HS_GATE_U1 = 23,
+  HS_GATE_U2 = 24,
+  HS_GATE_U3 = 25,
+  HS_GATE_RXX = 26,
+  HS_GATE_RYY = 27,
+  HS_GATE_RZZ = 28,
+  HS_GATE_TDG = 29,
+  HS_GATE_SDG = 30
+};
+
+#define HS_MAX_CONTROLS 5 /* MAX_CONTROL_QUBITS, types.hpp:8 */
+#define HS_MAX_TARGETS 5  /* MAX_TARGET_QUBITS, types.hpp:9  */
+
+/*
+ * One bound gate: the C form of SvSim::BoundGate (state_vector.hpp:1332-1379)
+ * = an AggregateGateFactory (basic_gates.hpp:1779) + controls + targets.
+ * `params` holds the constructor's complex arguments in order as (re, im)
+ * pairs: theta (1-param gates), phi, lambda (U2), theta, phi, lambda (U3),
+ * c00..c11 (C1), c00..c33 (C2).  Frac gates use frac_num / frac_pow
+ * (AggregateGate_Frac, basic_gates.hpp:1678).  sizeof == 320.
+ */
+typedef struct hs_gate {
+  int32_t type; /* enum hs_gate_type */
+  int32_t num_controls;
+  int32_t num_targets;
+  int32_t controls[HS_MAX_CONTROLS];
+  int32_t targets[HS_MAX_TARGETS];
+  uint32_t frac_num;
+  uint32_t frac_pow;
+  int32_t reserved;
+  double params[32];
+} hs_gate;
+
+typedef struct hs_state hs_state;
+
+/* ---- library ------------------------------------------------------------ */
+const char* hs_last_error(void);
+int hs_version(void);
+/* Number of CUDA devices visible (0 on a host without a GPU). */
+int hs_device_count(int* count);
+
+/* ---- state vector: StateVector (state_vector.hpp:41-1076) ------------------ */
+
+/* StateVector(n, numa) (py_wrapper.cpp:143, state_vector.hpp:60-119): a
+ * device-resident 2^n state initialised to |0...0>, identity slot map. */
+int hs_state_create(int num_qubits, int dtype, hs_state** out);
+int hs_state_destroy(hs_state* st);
+int hs_state_num_qubits(const hs_state* st, int* n);
+int hs_state_dtype(const hs_state* st, int* dtype);
+/* Device pointer of the slot-ordered amplitude array (for zero-copy users). */
+int hs_state_device_ptr(const hs_state* st, void** dptr);
+/* qubit_to_slot_ / slot_to_qubit_ (state_vector.hpp:146-150,250-265). */
+int hs_state_qubit_to_slot(const hs_state* st, int32_t* q2s /* [n] */);
+/* Set |x> (x in qubit order), identity slot map. */
+int hs_state_set_basis(hs_state* st, uint64_t x, void* stream);
+/* Copy `count` amplitudes starting at slot-ordered index `first`.
+ * `host` holds interleaved (re,im) of the state's dtype. */
+int hs_state_copy_to_host(hs_state* st, void* host, uint64_t first, uint64_t count,
+                          void* stream);
+int hs_state_copy_from_host(hs_state* st, const void* host, uint64_t first,
+                            uint64_t count, void* stream);
+/* Permute slots back to the identity map (qubit q in slot q) with K2 passes. */
+int hs_state_canonicalize(hs_state* st, void* stream);
+/* Convert between dtypes (c128 -> c64 rounding, c64 -> c128 widening); the two
+ * states must have the same qubit count; dst takes src's slot map. */
+int hs_state_convert(const hs_state* src, hs_state* dst, void* stream);
+
+/* ---- plain form (complex128 / complex64 state, per-gate arithmetic) -------- */
+
+/* BoundGate::apply (state_vector.hpp:1349 -> apply 402-510): one gate, one
+ * sweep over the state. */
+int hs_gate_apply(hs_state* st, const hs_gate* gate, void* stream);
+
+/* gather_and_execute_on (execute.hpp:171; live semantics of
+ * gather_and_execute_on_multi, execute.hpp:318-470): one part — every gate of
+ * `gates` applied in order inside one K1 launch that stages each 2^m tile of
+ * the state on chip and writes it back once. */
+int hs_part_run(hs_state* st, const hs_gate* gates, int num_gates, void* stream);
+
+/* Several parts back to back (the loop of execute_qasm_parts,
+ * qasm_assembler_standalone.py:1784-2018); part i is
+ * gates[part_offsets[i] .. part_offsets[i+1]). */
+int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
+                 int num_parts, void* stream);
+
+/* Tile-size override for K1 (0 = automatic).  Returns the previous value. */
+int hs_set_tile_qubits(int m);
+
+/* ---- redistribution (svsim-mpi.hpp:123-173, mpi_redistributer.hpp:100-344) */
+
+/* In-place bit-swap pass (K2): exchange slot bits pairs[2i] <-> pairs[2i+1]
+ * for all i (disjoint pairs).  Updates the slot map. */
+int hs_permute_bits(hs_state* st, const int32_t* pairs, int num_pairs, void* stream);
+
+/* SvSimMPI::gather_qubits semantics on one device (svsim-mpi.hpp:123-173 with
+ * gather_slots, mpi_redistributer.hpp:265-344): slots holding the qubits in
+ * `proc_qubits` become the top `num` slots (in current slot order) and all
+ * other qubits keep their relative order below them.  Done as at most two
+ * in-place involution passes of K2. */
+int hs_gather_qubits(hs_state* st, const int32_t* proc_qubits, int num, void* stream);
+
+/* ---- FP64 reductions (K3) ------------------------------------------------- */
+
+/* sum |a|^2 (is_normalized, state_vector.hpp:63-72) */
+int hs_norm2(hs_state* st, double* out);
+/* <a|b> = sum conj(a_i) b_i over qubit-aligned amplitudes (b is brought to
+ * a's slot map first if the maps differ). */
+int hs_inner(hs_state* a, hs_state* b, double out[2]);
+/* max_i |a_i - b_i| (state_equal / operator==, state_vector.hpp:1003-1072). */
+int hs_max_abs_diff(hs_state* a, hs_state* b, double* out);
+/* probability(qubit, value) (state_vector.hpp:897-923), race-free. */
+int hs_probability(hs_state* st, int qubit, int value, double* out);
+/* <Z_i Z_j> for num_pairs qubit pairs. */
+int hs_expect_zz(hs_state* st, const int32_t* pairs, int num_pairs, double* out);
+/* measure(qubits, num_samples) (state_vector.hpp:925-981) with a seeded
+ * generator: out[s*nq + j] = value of qubits[j] in sample s. */
+int hs_measure(hs_state* st, const int32_t* qubits, int num_qubits,
+               uint32_t num_samples, uint64_t seed, int32_t* out);
+
+/* ---- timers (py_wrapper.cpp:163-169) -------------------------------------- */
+/* Accumulated device time of K1/K2 launches in microseconds, and the number of
+ * gates / state passes issued since the last reset. */
+int hs_counters(long long* apply_us, long long* gate_count, long long* pass_count);
+int hs_counters_reset(void);
+/* Enable (1) or disable (0) device-time accounting for hs_counters; returns the
+ * previous setting. */
+int hs_set_timing(int on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HISV_H_ */
