@@ -1,0 +1,328 @@
+"""Benchmark: a 33-qubit, 40-layer random circuit on one B200.
+
+Workload (seeded synthetic stand-in for the reference's QASMBench-style
+circuits): 40 layers of U3 with uniform angles on every qubit followed by CZ
+on a random matching (33 is odd: one qubit idles per layer), 1960 gates,
+state |0...0>, acyclic parts of <= k qubits from hisvsim_b200.partition.
+
+A step simulates the whole circuit once.  `value` is the plain complex128
+form's throughput in amplitude updates per second (sum over gates of 2^n,
+divided by the circuit's device time); the circuit seconds and the HBM GB/s
+of the K1 passes ride along in the same line.  The state (128 GiB) is far
+larger than L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hisv|reference]
+
+Multi-GPU: replicas only (the path does not shard in this build); every rank
+simulates its own circuit, timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "33q circuit sec & HBM GB/s; fused FP32 vs plain FP64 GPU at 1-F≤1e-6"
+UNIT = "amp-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hisv", choices=["hisv", "reference"])
+    ap.add_argument("--qubits", type=int, default=33)
+    ap.add_argument("--layers", type=int, default=40)
+    ap.add_argument("--part-qubits", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-qubits", type=int, default=26, help="size of the CPU sample")
+    ap.add_argument("--cpu-layers", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---- distributed plumbing (replicas) ------------------------------------------
+
+def dist_setup(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def dist_max(pg, x):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ---- clocks --------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nme in enumerate(names):
+                if len(r) > 4 + i and r[4 + i].lower().startswith("active"):
+                    reasons.add(nme)
+        loaded = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# ---- workload ------------------------------------------------------------------
+
+def workload(n, layers, seed, k):
+    from hisvsim_b200 import circuits, partition
+    from hisvsim_b200.gates import part_offsets
+
+    gates = circuits.random_u3_cz(n, layers, seed)
+    parts = partition.partition_acyclic(gates, k)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    return gates, parts, rec, offs
+
+
+def cpu_sample(args, threads):
+    """The reference's own CPU path (oracle/_ref, BoundGate::apply per gate and
+    gather_and_execute_on_multi per part) on a bounded sample of the workload."""
+    from oracle.oracle import RefOracle
+
+    n, layers = args.cpu_qubits, args.cpu_layers
+    gates, parts, rec, offs = workload(n, layers, args.seed, min(args.part_qubits, n))
+    from hisvsim_b200.gates import to_records
+
+    ref = RefOracle()
+    flat = to_records(gates)
+    t = time.perf_counter()
+    ref.run(n, flat, mode=0, threads=threads)
+    t_gate = time.perf_counter() - t
+    upd = len(gates) * float(1 << n)
+    return {"value": upd / t_gate, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n} qubits x {layers} layers of the same circuit family "
+                      f"({len(gates)} gates), per-gate BoundGate::apply "
+                      f"(state_vector.hpp:1349), {t_gate:.2f} s",
+            "seconds": t_gate}
+
+
+def run_reference_arm(args):
+    # a CPU-only arm: rank 0 alone times the reference; other ranks exit at once
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(args, threads)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic",
+            "config": {"workload": f"random U3+CZ circuit, CPU sample {args.cpu_qubits}q x "
+                                   f"{args.cpu_layers} layers (33q x 40 layers needs 128 GiB "
+                                   f"and ~2 h of CPU per step)",
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    rank, world, local, pg = dist_setup(args.gpus)
+    from hisvsim_b200 import abi
+
+    abi.set_device(local)
+    n = args.qubits
+    gates, parts, rec, offs = workload(n, args.layers, args.seed + rank, args.part_qubits)
+    upd = len(gates) * float(1 << n)
+
+    st = abi.State(n, abi.C128)
+    start, stop = abi.Event(), abi.Event()
+
+    def step():
+        st.set_basis(0)
+        st.run_parts(rec, offs)
+
+    for _ in range(args.warmup):
+        step()
+    abi.synchronize()
+    abi.counters_reset()
+    abi.set_timing(True)
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        abi.synchronize()
+        start.record()
+        for _ in range(args.steps):
+            step()
+        stop.record()
+        ms = start.elapsed_ms(stop)
+    abi.set_timing(False)
+    c = abi.counters()
+    pbytes = abi.launch_bytes()
+    t_step = dist_max(pg, ms / 1e3 / args.steps)
+    passes = c["passes"] / args.steps
+    k1_avg_ms = c["apply_us"] / 1e3 / max(1, c["passes"])
+    bytes_per_pass = 2.0 * (1 << n) * 16
+    norm = st.norm2()
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak_gbs, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak_gbs, peak_src = 6650.0, "fallback"
+    k1_gbs = bytes_per_pass / (k1_avg_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "k1_traffic.json")))
+        traffic = tr.get("bytes_per_launch_scaled_33q")
+    except Exception:
+        pass
+
+    # end to end through the public API (pybind module): allocate, run every
+    # part from host gate lists, read back the norm
+    e2e = None
+    if not args.no_e2e:
+        del st
+        from hisvsim_b200 import svsimulator_py_wrapper as svsim
+        from hisvsim_b200.gates import NOPARAM
+
+        def bound(g):
+            if g.name in NOPARAM:
+                ag = svsim.AggregateGate_0(g.name)
+            else:
+                ag = svsim.AggregateGate_3(g.name, *g.params)
+            return svsim.BoundGate(svsim.AggregateGateFactory(ag), list(g.controls),
+                                   list(g.targets))
+
+        lists = [[bound(gates[i]) for i in p] for p in parts]
+        abi.counters_reset()
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(max(1, min(args.steps, 2))):
+            sim = svsim.StateVector(n, 0)
+            for bl in lists:
+                svsim.gather_and_execute_on(sim, bl)
+            _ = sim.norm()
+            del sim
+        e2e_steps = max(1, min(args.steps, 2))
+        t_e2e = dist_max(pg, (time.perf_counter() - t0) / e2e_steps)
+        e2e = {"value": world * upd / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": abi.launch_bytes() // e2e_steps,
+               "d2h_bytes_per_step": 16, "circuit_s": t_e2e,
+               "path": "svsimulator_py_wrapper: StateVector -> gather_and_execute_on per part "
+                       "-> norm readback"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_sample(args, os.cpu_count() or 1)
+        except Exception as ex:  # the oracle library may be missing
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * upd / t_step, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic",
+            "config": {"workload": f"random circuit {n} qubits x {args.layers} layers "
+                                   f"(U3 all qubits + CZ random matching), plain complex128",
+                       "gates": len(gates), "parts": len(parts),
+                       "part_qubits": args.part_qubits, "passes_per_step": passes,
+                       "state_bytes": (1 << n) * 16, "l2": "state 128 GiB >> L2, no flush",
+                       "parallelism": f"replicas{world}"},
+            "circuit_s": t_step, "hbm_GBps": passes * bytes_per_pass / t_step / 1e9,
+            "hbm_frac": passes * bytes_per_pass / t_step / 1e9 / peak_gbs,
+            "norm": norm,
+            "roofline": {"bound": "hbm", "achieved": k1_gbs, "peak": peak_gbs, "unit": "GB/s",
+                         "frac": k1_gbs / peak_gbs, "traffic": traffic, "peak_source": peak_src,
+                         "kernel": "k1_part", "algorithmic_bytes_per_launch": bytes_per_pass,
+                         "avg_launch_ms": k1_avg_ms},
+            "gpu_launches": int(c["passes"] + args.steps),
+            "launch_param_bytes_per_step": pbytes / args.steps,
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

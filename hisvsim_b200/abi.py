@@ -41,6 +41,13 @@ SIGNATURES = {
     "hs_last_error": [],
     "hs_version": [],
     "hs_device_count": [ctypes.POINTER(_i)],
+    "hs_device_set": [_i],
+    "hs_device_synchronize": [],
+    "hs_event_create": [ctypes.POINTER(_vp)],
+    "hs_event_record": [_vp, _vp],
+    "hs_event_elapsed_ms": [_vp, _vp, ctypes.POINTER(ctypes.c_float)],
+    "hs_event_destroy": [_vp],
+    "hs_launch_bytes": [_llp],
     "hs_state_create": [_i, _i, ctypes.POINTER(_vp)],
     "hs_state_destroy": [_vp],
     "hs_state_num_qubits": [_vp, ctypes.POINTER(_i)],
@@ -222,6 +229,47 @@ class State:
         out = np.zeros((nsamples, len(q)), dtype=np.int32)
         check(lib().hs_measure(self.h, _ptr(q), len(q), nsamples, seed, _ptr(out)))
         return out
+
+
+def set_device(d: int):
+    check(lib().hs_device_set(d))
+
+
+def synchronize():
+    check(lib().hs_device_synchronize())
+
+
+class Event:
+    """A CUDA event recorded on the library's stream (NULL = legacy default)."""
+
+    def __init__(self):
+        h = _vp()
+        check(lib().hs_event_create(ctypes.byref(h)))
+        self.h = h
+
+    def record(self, stream=None):
+        check(lib().hs_event_record(self.h, stream))
+
+    def elapsed_ms(self, end: "Event") -> float:
+        ms = ctypes.c_float()
+        check(lib().hs_event_elapsed_ms(self.h, end.h, ctypes.byref(ms)))
+        return ms.value
+
+    def __del__(self):
+        try:
+            lib().hs_event_destroy(self.h)
+        except Exception:
+            pass
+
+
+def launch_bytes() -> int:
+    b = ctypes.c_longlong()
+    check(lib().hs_launch_bytes(ctypes.byref(b)))
+    return b.value
+
+
+def set_timing(on: bool) -> int:
+    return lib().hs_set_timing(1 if on else 0)
 
 
 def set_tile_qubits(m: int) -> int:

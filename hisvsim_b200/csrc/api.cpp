@@ -23,7 +23,7 @@ int set_error(int code, const char* fmt, ...) {
   return code;
 }
 
-static std::atomic<long long> g_gates{0}, g_passes{0};
+static std::atomic<long long> g_gates{0}, g_passes{0}, g_param_bytes{0};
 static std::atomic<int> g_tile_hint{0};
 
 // device-time accounting of K1/K2 launches: event pairs resolved when read
@@ -113,6 +113,7 @@ int run_lowered(hs_state* st, const std::vector<LoweredGate>& lg, long long ngat
   for (const auto& p : progs) {
     HS_TRY(launch_part(st->amp, st->dtype, p, s));
     count_pass(p.nops);
+    g_param_bytes += (long long)sizeof(PartProgram);
   }
   (void)ngates;
   return HS_OK;
@@ -139,6 +140,40 @@ int hs_device_count(int* count) {
   cudaError_t e = cudaGetDeviceCount(&c);
   if (e != cudaSuccess) c = 0;
   if (count) *count = c;
+  return HS_OK;
+}
+
+int hs_device_set(int device) {
+  HS_CUDA(cudaSetDevice(device));
+  return HS_OK;
+}
+
+int hs_device_synchronize(void) {
+  HS_CUDA(cudaDeviceSynchronize());
+  return HS_OK;
+}
+
+int hs_event_create(void** ev) {
+  cudaEvent_t e;
+  HS_CUDA(cudaEventCreate(&e));
+  *ev = e;
+  return HS_OK;
+}
+
+int hs_event_record(void* ev, void* stream) {
+  HS_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(ev), S(stream)));
+  return HS_OK;
+}
+
+int hs_event_elapsed_ms(void* start, void* stop, float* ms) {
+  HS_CUDA(cudaEventSynchronize(static_cast<cudaEvent_t>(stop)));
+  HS_CUDA(cudaEventElapsedTime(ms, static_cast<cudaEvent_t>(start),
+                               static_cast<cudaEvent_t>(stop)));
+  return HS_OK;
+}
+
+int hs_event_destroy(void* ev) {
+  if (ev) cudaEventDestroy(static_cast<cudaEvent_t>(ev));
   return HS_OK;
 }
 
@@ -481,6 +516,12 @@ int hs_counters_reset(void) {
   g_apply_us = 0;
   g_gates = 0;
   g_passes = 0;
+  g_param_bytes = 0;
+  return HS_OK;
+}
+
+int hs_launch_bytes(long long* bytes) {
+  if (bytes) *bytes = g_param_bytes.load();
   return HS_OK;
 }
 

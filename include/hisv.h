@@ -111,6 +111,16 @@ const char* hs_last_error(void);
 int hs_version(void);
 /* Number of CUDA devices visible (0 on a host without a GPU). */
 int hs_device_count(int* count);
+/* Select the device used by this thread's subsequent calls (one process per
+ * GPU: rank r calls hs_device_set(local_rank)). */
+int hs_device_set(int device);
+int hs_device_synchronize(void);
+
+/* ---- device timing (CUDA events on the caller's stream) ------------------- */
+int hs_event_create(void** ev);
+int hs_event_record(void* ev, void* stream);
+int hs_event_elapsed_ms(void* start, void* stop, float* ms); /* waits for stop */
+int hs_event_destroy(void* ev);
 
 /* ---- state vector: StateVector (state_vector.hpp:41-1076) ------------------ */
 
@@ -195,6 +205,9 @@ int hs_measure(hs_state* st, const int32_t* qubits, int num_qubits,
  * gates / state passes issued since the last reset. */
 int hs_counters(long long* apply_us, long long* gate_count, long long* pass_count);
 int hs_counters_reset(void);
+/* Bytes of kernel parameters (gate programs) sent with K1/K2 launches since
+ * the last counter reset: the host-to-device traffic of a circuit. */
+int hs_launch_bytes(long long* bytes);
 /* Enable (1) or disable (0) device-time accounting for hs_counters; returns the
  * previous setting. */
 int hs_set_timing(int on);

@@ -1,0 +1,134 @@
+"""Host-side checks that need no GPU: the C ABI library and its exports, the
+pybind11 module's API surface and error behaviour, partitioners and the
+part-file format, circuit generators."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from hisvsim_b200 import abi, circuits, partition
+from hisvsim_b200.gates import HS_GATE_DTYPE, Gate, to_records
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "hisv.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(hs_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.lib()
+    names = header_functions()
+    assert len(names) >= 29
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_signatures_cover_header():
+    assert set(header_functions()) <= set(abi.SIGNATURES)
+
+
+def test_gate_record_layout(port):
+    assert HS_GATE_DTYPE.itemsize == 320 == port.gate_size
+
+
+def test_version_and_errors_without_device():
+    assert abi.lib().hs_version() >= 1
+    if abi.device_count() == 0:
+        with pytest.raises(abi.HisvError) as e:
+            abi.State(4)
+        assert e.value.code == abi.HS_E_NODEVICE
+
+
+def test_null_state_is_an_error():
+    rc = abi.lib().hs_norm2(None, ctypes.byref(ctypes.c_double()))
+    assert rc == abi.HS_E_INVALID
+    assert b"null" in abi.lib().hs_last_error()
+
+
+def test_tile_hint_bounds():
+    assert abi.lib().hs_set_tile_qubits(99) == abi.HS_E_INVALID
+    prev = abi.set_tile_qubits(11)
+    assert abi.set_tile_qubits(prev) == 11
+
+
+def test_pymod_surface():
+    from hisvsim_b200 import svsimulator_py_wrapper as sv
+
+    for name in ["AggregateGate_0", "AggregateGate_1", "AggregateGate_2", "AggregateGate_3",
+                 "AggregateGate_C1", "AggregateGate_C2", "AggregateGate_Frac",
+                 "AggregateGateFactory", "StateVector", "BoundGate", "gather_and_execute_on",
+                 "obtain_apply_time", "obtain_gate_counter", "obtain_move_counter",
+                 "obtain_gather_time", "set_num_threads", "set_init_num_threads",
+                 "set_opt_slots"]:
+        assert hasattr(sv, name), name
+    ag = sv.AggregateGate_3("u3", 0.1, 0.2, 0.3)
+    b = sv.BoundGate(sv.AggregateGateFactory(ag), [1], [0])
+    assert b is not None
+    # names the reference cannot build raise instead of aborting
+    with pytest.raises(ValueError):
+        sv.AggregateGate_0("RX")
+    with pytest.raises(ValueError):
+        sv.AggregateGate_1("NOPE", 1.0)
+    with pytest.raises(ValueError):
+        sv.AggregateGate_Frac("RZFrac", 1, 2)  # mixed-case table entry never matches
+    with pytest.raises(ValueError):
+        sv.BoundGate(sv.AggregateGateFactory(sv.AggregateGate_0("X")), [1, 2, 3, 4, 5, 6], [0])
+
+
+@pytest.mark.parametrize("strategy", [partition.partition_acyclic, partition.partition_natural,
+                                      partition.partition_dfs])
+@pytest.mark.parametrize("k", [2, 4, 7])
+def test_partitions_valid(strategy, k):
+    gates = circuits.random_layered(12, 5, 4)
+    parts = strategy(gates, k)
+    assert partition.is_valid_partition(gates, parts)
+    for p in parts:
+        assert len({q for i in p for q in gates[i].qubits}) <= k
+
+
+def test_acyclic_beats_natural():
+    gates = circuits.random_u3_cz(20, 10, 1)
+    a = partition.partition_acyclic(gates, 6)
+    b = partition.partition_natural(gates, 6)
+    assert len(a) <= len(b)
+
+
+def test_part_file_roundtrip(tmp_path):
+    gates = circuits.random_layered(8, 3, 2)
+    parts = partition.partition_acyclic(gates, 4)
+    f = tmp_path / "c_part_smart"
+    partition.write_part_file(str(f), gates, parts)
+    assert partition.read_part_file(str(f), len(gates)) == parts
+    # order id 0 and ids beyond the gate list are skipped (parse rules of the reference driver)
+    with open(f, "a") as fh:
+        fh.write(f"0 start 0\n{len(gates) + 2000} exit 1\n")
+    assert partition.read_part_file(str(f), len(gates)) == parts
+
+
+def test_partition_rejects_oversized_gate():
+    with pytest.raises(ValueError):
+        partition.partition_acyclic([Gate("X", (0,), (1, 2))], 2)
+
+
+def test_generators_shapes():
+    g = circuits.random_layered(20, 20, 0)
+    assert len(g) == 20 * (20 + 10)
+    g2 = circuits.random_u3_cz(33, 40, 0)
+    assert len(g2) == 40 * (33 + 16)
+    q, x = circuits.qft(30, 1)
+    assert len(q) == 30 + 30 * 29 // 2 + 15 and 0 <= x < 2 ** 30
+    qa, edges, gam, bet = circuits.qaoa_maxcut(16, 4, 9)
+    assert len(edges) == 24 and all(d == 3 for d in np.bincount(np.ravel(edges)))
+    assert circuits.random_layered(10, 3, 5) == circuits.random_layered(10, 3, 5)
+
+
+def test_records_roundtrip():
+    gates = [Gate("U3", (3,), (1, 2), params=(0.1, 0.2, 0.3)), Gate("R1FRAC", (0,), frac=(3, 4))]
+    r = to_records(gates)
+    assert r["type"].tolist() == [25, 19]
+    assert r["controls"][0][:2].tolist() == [1, 2]
+    assert r["frac_num"][1] == 3 and r["frac_pow"][1] == 4
