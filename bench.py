@@ -42,12 +42,13 @@ def parse():
     ap.add_argument("--impl", default="hisv", choices=["hisv", "reference"])
     ap.add_argument("--qubits", type=int, default=33)
     ap.add_argument("--layers", type=int, default=40)
-    ap.add_argument("--part-qubits", type=int, default=10)
+    ap.add_argument("--part-qubits", type=int, default=9)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-qubits", type=int, default=26, help="size of the CPU sample")
     ap.add_argument("--cpu-layers", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tile-qubits", type=int, default=11, help="K1 tile bits (0 = automatic)")
     return ap.parse_args()
 
 
@@ -205,6 +206,8 @@ def main():
     from hisvsim_b200 import abi
 
     abi.set_device(local)
+    if args.tile_qubits:
+        abi.set_tile_qubits(args.tile_qubits)
     n = args.qubits
     gates, parts, rec, offs = workload(n, args.layers, args.seed + rank, args.part_qubits)
     upd = len(gates) * float(1 << n)

@@ -63,6 +63,7 @@ SIGNATURES = {
     "hs_part_run": [_vp, _vp, _i, _vp],
     "hs_parts_run": [_vp, _vp, _vp, _i, _vp],
     "hs_set_tile_qubits": [_i],
+    "hs_plan_stats": [_i, _i, _vp, _i, _vp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
@@ -229,6 +230,14 @@ class State:
         out = np.zeros((nsamples, len(q)), dtype=np.int32)
         check(lib().hs_measure(self.h, _ptr(q), len(q), nsamples, seed, _ptr(out)))
         return out
+
+
+def plan_stats(n: int, gates, dtype: int = C128) -> dict:
+    """Host-only K1 planning statistics of one part (no GPU needed)."""
+    rec = _records(gates)
+    out = np.zeros(6, dtype=np.int32)
+    check(lib().hs_plan_stats(n, dtype, _ptr(rec), len(rec), _ptr(out)))
+    return dict(zip(["passes", "groups", "ops", "dense", "diag", "tile_bits"], out.tolist()))
 
 
 def set_device(d: int):

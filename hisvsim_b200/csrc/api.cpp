@@ -108,7 +108,7 @@ int permute_positions(hs_state* st, const std::vector<int>& pi, cudaStream_t s) 
 int run_lowered(hs_state* st, const std::vector<LoweredGate>& lg, long long ngates,
                 cudaStream_t s) {
   std::vector<PartProgram> progs;
-  HS_TRY(plan_part(st->n, st->q2s, lg, g_tile_hint.load(), &progs));
+  HS_TRY(plan_part(st->n, st->q2s, lg, g_tile_hint.load(), st->dtype, &progs));
   TimedRegion tr(s);
   for (const auto& p : progs) {
     HS_TRY(launch_part(st->amp, st->dtype, p, s));
@@ -334,6 +334,35 @@ int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets
                      &all[p]));
   for (int p = 0; p < num_parts; ++p)
     HS_TRY(run_lowered(st, all[p], part_offsets[p + 1] - part_offsets[p], S(stream)));
+  return HS_OK;
+}
+
+int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates,
+                  int32_t* stats) {
+  if (num_qubits < 1 || num_qubits > 40) return set_error(HS_E_INVALID, "bad qubit count");
+  if (dtype != HS_DTYPE_C128 && dtype != HS_DTYPE_C64) return set_error(HS_E_INVALID, "bad dtype");
+  std::vector<LoweredGate> lg(num_gates);
+  for (int i = 0; i < num_gates; ++i) HS_TRY(lower_gate(gates[i], num_qubits, &lg[i]));
+  std::vector<int> q2s(num_qubits);
+  for (int q = 0; q < num_qubits; ++q) q2s[q] = q;
+  std::vector<PartProgram> progs;
+  HS_TRY(plan_part(num_qubits, q2s, lg, g_tile_hint.load(), dtype, &progs));
+  int32_t groups = 0, ops = 0, diag = 0, dense = 0, m = 0;
+  for (const auto& p : progs) {
+    groups += p.ngroups;
+    ops += p.nops;
+    m = std::max(m, int(p.m));
+    for (int i = 0; i < p.nops; ++i) {
+      diag += p.ops[i].kind >= OPD_PHASE;
+      dense += p.ops[i].kind == OP1_DENSE || p.ops[i].kind == OP2_DENSE;
+    }
+  }
+  stats[0] = int32_t(progs.size());
+  stats[1] = groups;
+  stats[2] = ops;
+  stats[3] = dense;
+  stats[4] = diag;
+  stats[5] = m;
   return HS_OK;
 }
 

@@ -46,35 +46,47 @@ int lower_gate(const hs_gate& g, int num_qubits, LoweredGate* out);
 // ---- K1 part program --------------------------------------------------------
 constexpr int kRegBits = 4;        // amplitudes per thread = 2^kRegBits
 constexpr int kMaxTileBits = 13;   // 2^13 complex128 = 128 KiB of shared memory
-constexpr int kMaxOps = 160;
+constexpr int kMaxOps = 128;
 constexpr int kMaxCoef = 640;      // complex coefficients (double2)
 constexpr int kMaxGroups = 48;
 constexpr int kMaxRuns = 16;
 
 enum OpKind : uint8_t {
+  // gates whose targets must be register bits
   OP1_DENSE = 0,  // 2x2
-  OP1_DIAG = 1,   // diag(d0, d1)
-  OP1_PHASE = 2,  // diag(1, d1)
-  OP1_NEG = 3,    // diag(1, -1)
-  OP1_X = 4,      // [[0,1],[1,0]]
-  OP1_H = 5,      // s*[[1,1],[1,-1]], s = 1/sqrt(2)
-  OP1_Y = 6,      // [[0,-i],[i,0]]
-  OP2_DENSE = 8,  // 4x4
-  OP2_DIAG = 9,   // diag(4)
-  OP2_SWAP = 10,  // swap |01>,|10>
+  OP1_X = 1,      // [[0,1],[1,0]]
+  OP1_H = 2,      // s*[[1,1],[1,-1]], s = 1/sqrt(2)
+  OP1_Y = 3,      // [[0,-i],[i,0]]
+  OP2_DENSE = 4,  // 4x4
+  OP2_SWAP = 5,   // swap |01>,|10>
+  // diagonal gates: targets anywhere (register, thread or outer bits)
+  OPD_PHASE = 8,  // multiply by c0 where every bit of the mask is 1
+  OPD_NEG = 9,    // negate where every bit of the mask is 1
+  OPD_DIAG = 10,  // multiply by c[b0 | b1 << 1] where the control mask holds
 };
+// dispatch codes (kernel switch):
+//   1q dense, uncontrolled (v -> other array):      0 + ja           (0..3)
+//   1q dense, controlled (in place):                 4 + ja           (4..7)
+//   diagonal sign flip, register mask p (in place): 16 + p           (16..31)
+//   diagonal phase, register mask p (in place):     32 + p           (32..47)
+//   general diagonal (in place):                    48
+//   2q dense, uncontrolled (v -> other array):      64 + pair        (64..69)
+//   2q dense, controlled (in place):                72 + pair        (72..77)
+//   2q swap (in place):                             80 + pair        (80..85)
+enum TargetWhere : uint8_t { TW_NONE = 0, TW_REG = 1, TW_THR = 2, TW_OUT = 3 };
 
 struct DevOp {
   uint8_t kind;
-  uint8_t ja, jb;     // register-bit positions of the targets (ja < jb for 2q)
-  uint8_t pad;
-  uint16_t coef;      // first coefficient (index into PartProgram::coef)
-  uint16_t creg;      // controls that are register bits, in register-element space
-  uint32_t cthr;      // controls that are thread bits, in tile-index space
-  uint32_t pad2;
-  uint64_t couter;    // controls outside the tile, in global-index space
+  uint8_t code;
+  uint8_t ja, jb;             // register positions of non-diagonal targets (ja < jb)
+  uint8_t t0w, t0p, t1w, t1p;  // diagonal targets: where (TargetWhere) and position
+  uint16_t coef;              // first coefficient (index into PartProgram::coef)
+  uint16_t creg;              // control/mask bits that are register bits (element space)
+  uint32_t cthr;              // control/mask bits that are thread bits (tile-index space)
+  uint64_t couter;            // control/mask bits outside the tile (global index space)
+  uint64_t pad;
 };
-static_assert(sizeof(DevOp) == 24, "DevOp layout");
+static_assert(sizeof(DevOp) == 32, "DevOp layout");
 
 struct Runs {  // bit-run deposit: out |= ((x >> src) & (2^len - 1)) << dst
   uint8_t n;
@@ -99,6 +111,7 @@ struct PartProgram {
   uint64_t ntiles;     // 2^(n-m)
   Runs tile;           // tile index -> global index
   Runs outer;          // tile number -> global index
+  uint8_t tile_slot[16];  // global slot of tile bit b
   GroupDesc groups[kMaxGroups];
   DevOp ops[kMaxOps];
   double2 coef[kMaxCoef];
@@ -109,7 +122,8 @@ static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
 // qubit q sits in slot q2s[q].  Long parts produce several programs (each one
 // state pass).  Returns HS_OK or an error.
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
-              int tile_bits_hint, std::vector<PartProgram>* programs);
+              int tile_bits_hint, int dtype, std::vector<PartProgram>* programs);
+inline int max_tile_bits(int dtype) { (void)dtype; return 12; }
 
 // ---- K2 bit-swap program ----------------------------------------------------
 struct PermProgram {

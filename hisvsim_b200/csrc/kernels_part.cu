@@ -75,195 +75,362 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
 }
 
 // ---- gate bodies on registers ------------------------------------------------
+// Each thread holds its amplitudes in one of two register arrays.  Uncontrolled
+// dense gates write the other array (all of its elements), so no register is
+// copied back after a gate; the op interpreter is a two-state machine that
+// tracks which array holds the data.  Controlled dense gates and diagonal
+// gates update the current array in place; sign flips and phases are
+// specialized by their register mask so only the affected elements are
+// touched.
 
+template <int J>
+__device__ __forceinline__ constexpr int ins0(int p) {  // insert a 0 bit at J
+  return ((p >> J) << (J + 1)) | (p & ((1 << J) - 1));
+}
+
+__device__ __forceinline__ double flip_sign(double x, uint32_t sm) {
+  return __hiloint2double(__double2hiint(x) ^ int(sm), __double2loint(x));
+}
+__device__ __forceinline__ float flip_sign(float x, uint32_t sm) {
+  return __int_as_float(__float_as_int(x) ^ int(sm));
+}
+
+// dense 2x2 on register bit J, src -> dst
 template <int R, int J, typename V>
-__device__ __forceinline__ void apply1(V (&v)[1 << R], const DevOp& op, const double2* coef,
-                                       bool thr_ok) {
+__device__ __forceinline__ void d1x(const V (&s)[1 << R], V (&d)[1 << R], const double2* __restrict__ c) {
   constexpr int E = 1 << R;
-  const uint32_t creg = op.creg;
+  const double2 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
 #pragma unroll
   for (int p = 0; p < E / 2; ++p) {
-    const int e0 = ((p >> J) << (J + 1)) | (p & ((1 << J) - 1));
-    const int e1 = e0 | (1 << J);
-    if (!thr_ok || ((uint32_t(e0) & creg) != creg)) continue;
-    V a = v[e0], b = v[e1];
-    switch (op.kind) {
-      case OP1_DENSE:
-        v[e0] = cmac2(coef[0], a, coef[1], b);
-        v[e1] = cmac2(coef[2], a, coef[3], b);
-        break;
-      case OP1_DIAG:
-        v[e0] = cmul(coef[0], a);
-        v[e1] = cmul(coef[1], b);
-        break;
-      case OP1_PHASE:
-        v[e1] = cmul(coef[0], b);
-        break;
-      case OP1_NEG:
-        v[e1] = mk<V>(-b.x, -b.y);
-        break;
-      case OP1_X:
-        v[e0] = b;
-        v[e1] = a;
-        break;
-      case OP1_H: {
-        using T = typename Scalar<V>::T;
-        const T s = T(0.707106781186547524401);
-        v[e0] = mk<V>(s * (a.x + b.x), s * (a.y + b.y));
-        v[e1] = mk<V>(s * (a.x - b.x), s * (a.y - b.y));
-        break;
-      }
-      case OP1_Y:  // [[0,-i],[i,0]]
-        v[e0] = mk<V>(b.y, -b.x);
-        v[e1] = mk<V>(-a.y, a.x);
-        break;
-      default:
-        break;
+    const int e0 = ins0<J>(p), e1 = e0 | (1 << J);
+    d[e0] = cmac2(c0, s[e0], c1, s[e1]);
+    d[e1] = cmac2(c2, s[e0], c3, s[e1]);
+  }
+}
+
+// dense 2x2 on register bit J, in place, for pairs whose controls hold
+template <int R, int J, typename V>
+__device__ __forceinline__ void d1c(V (&v)[1 << R], const double2* __restrict__ c, uint32_t creg,
+                                    bool ok) {
+  constexpr int E = 1 << R;
+  const double2 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3];
+#pragma unroll
+  for (int p = 0; p < E / 2; ++p) {
+    const int e0 = ins0<J>(p), e1 = e0 | (1 << J);
+    if (!ok || (uint32_t(e0) & creg) != creg) continue;
+    const V a = v[e0], b = v[e1];
+    v[e0] = cmac2(c0, a, c1, b);
+    v[e1] = cmac2(c2, a, c3, b);
+  }
+}
+
+// sign flip of the elements whose register bits cover mask M (sm = 0 or sign bit)
+template <int R, int M, typename V>
+__device__ __forceinline__ void dneg(V (&v)[1 << R], uint32_t sm) {
+  constexpr int E = 1 << R;
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if ((e & M) == M) {
+      v[e].x = flip_sign(v[e].x, sm);
+      v[e].y = flip_sign(v[e].y, sm);
+    }
+}
+
+// multiply the elements whose register bits cover mask M by f (in place)
+template <int R, int M, typename V>
+__device__ __forceinline__ void dphase(V (&v)[1 << R], double2 f) {
+  using T = typename Scalar<V>::T;
+  constexpr int E = 1 << R;
+  const T fx = T(f.x), fy = T(f.y);
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    if ((e & M) == M) {
+      const T a = fy * v[e].y, b = fy * v[e].x;
+      v[e].x = fma(fx, v[e].x, -a);
+      v[e].y = fma(fx, v[e].y, b);
+    }
+}
+
+// general diagonal: coefficient c[b0 | b1 << 1] with its target bits read from
+// register, thread or outer bits (in place)
+template <int R, typename V>
+__device__ __forceinline__ void ddiag(V (&v)[1 << R], const DevOp& op, const double2* __restrict__ c,
+                                      uint32_t thr, uint64_t gbase, bool ok) {
+  constexpr int E = 1 << R;
+  const uint32_t creg = ok ? uint32_t(op.creg) : 0xffffffffu;
+  auto fixed = [&](uint8_t w, uint8_t pos) -> uint32_t {
+    return w == TW_THR ? ((thr >> pos) & 1u) : w == TW_OUT ? uint32_t((gbase >> pos) & 1ull) : 0u;
+  };
+  const uint32_t f0 = fixed(op.t0w, op.t0p), f1 = fixed(op.t1w, op.t1p) << 1;
+  const bool r0 = op.t0w == TW_REG, r1 = op.t1w == TW_REG;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    if ((uint32_t(e) & creg) != creg) continue;
+    const uint32_t q0 = r0 ? ((uint32_t(e) >> op.t0p) & 1u) : f0;
+    const uint32_t q1 = r1 ? (((uint32_t(e) >> op.t1p) & 1u) << 1) : f1;
+    v[e] = cmul(c[q0 | q1], v[e]);
+  }
+}
+
+// dense 4x4 on register bits JA < JB, src -> dst
+template <int R, int JA, int JB, typename V>
+__device__ __forceinline__ void d2x(const V (&s)[1 << R], V (&d)[1 << R], const double2* __restrict__ c) {
+  constexpr int E = 1 << R;
+#pragma unroll
+  for (int p = 0; p < E / 4; ++p) {
+    const int x = ins0<JB>(ins0<JA>(p));
+    const int e[4] = {x, x | (1 << JA), x | (1 << JB), x | (1 << JA) | (1 << JB)};
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const V t0 = cmac2(c[4 * r], s[e[0]], c[4 * r + 1], s[e[1]]);
+      const V t1 = cmac2(c[4 * r + 2], s[e[2]], c[4 * r + 3], s[e[3]]);
+      d[e[r]] = mk<V>(t0.x + t1.x, t0.y + t1.y);
     }
   }
 }
 
-template <int R, int JA, int JB, typename V>
-__device__ __forceinline__ void apply2(V (&v)[1 << R], const DevOp& op, const double2* coef,
-                                       bool thr_ok) {
+// 4x4 dense (controlled) or swap, in place
+template <int R, int JA, int JB, bool SWAP, typename V>
+__device__ __forceinline__ void d2c(V (&v)[1 << R], const double2* __restrict__ c, uint32_t creg,
+                                    bool ok) {
   constexpr int E = 1 << R;
-  const uint32_t creg = op.creg;
 #pragma unroll
   for (int p = 0; p < E / 4; ++p) {
-    // insert zero bits at JA (< JB) and JB
-    int x = ((p >> JA) << (JA + 1)) | (p & ((1 << JA) - 1));
-    x = ((x >> JB) << (JB + 1)) | (x & ((1 << JB) - 1));
+    const int x = ins0<JB>(ins0<JA>(p));
     const int e[4] = {x, x | (1 << JA), x | (1 << JB), x | (1 << JA) | (1 << JB)};
-    if (!thr_ok || ((uint32_t(x) & creg) != creg)) continue;
-    if (op.kind == OP2_SWAP) {
-      V t = v[e[1]];
+    if (!ok || (uint32_t(x) & creg) != creg) continue;
+    if (SWAP) {
+      const V t = v[e[1]];
       v[e[1]] = v[e[2]];
       v[e[2]] = t;
-    } else if (op.kind == OP2_DIAG) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) v[e[k]] = cmul(coef[k], v[e[k]]);
     } else {
-      V a[4] = {v[e[0]], v[e[1]], v[e[2]], v[e[3]]};
+      const V a[4] = {v[e[0]], v[e[1]], v[e[2]], v[e[3]]};
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        V t0 = cmac2(coef[4 * r], a[0], coef[4 * r + 1], a[1]);
-        V t1 = cmac2(coef[4 * r + 2], a[2], coef[4 * r + 3], a[3]);
+        const V t0 = cmac2(c[4 * r], a[0], c[4 * r + 1], a[1]);
+        const V t1 = cmac2(c[4 * r + 2], a[2], c[4 * r + 3], a[3]);
         v[e[r]] = mk<V>(t0.x + t1.x, t0.y + t1.y);
       }
     }
   }
 }
 
-template <int R, typename V>
-__device__ __forceinline__ void apply_op(V (&v)[1 << R], const DevOp& op, const double2* coef,
-                                         bool thr_ok) {
-  if (op.kind < OP2_DENSE) {
-    switch (op.ja) {
-      case 0: apply1<R, 0>(v, op, coef, thr_ok); break;
-      case 1: if constexpr (R > 1) apply1<R, 1>(v, op, coef, thr_ok); break;
-      case 2: if constexpr (R > 2) apply1<R, 2>(v, op, coef, thr_ok); break;
-      case 3: if constexpr (R > 3) apply1<R, 3>(v, op, coef, thr_ok); break;
-      default: break;
-    }
-  } else if constexpr (R >= 2) {
-    const int key = op.ja * 4 + op.jb;
-    switch (key) {
-      case 1: apply2<R, 0, 1>(v, op, coef, thr_ok); break;
-      case 2: if constexpr (R > 2) apply2<R, 0, 2>(v, op, coef, thr_ok); break;
-      case 3: if constexpr (R > 3) apply2<R, 0, 3>(v, op, coef, thr_ok); break;
-      case 6: if constexpr (R > 2) apply2<R, 1, 2>(v, op, coef, thr_ok); break;
-      case 7: if constexpr (R > 3) apply2<R, 1, 3>(v, op, coef, thr_ok); break;
-      case 11: if constexpr (R > 3) apply2<R, 2, 3>(v, op, coef, thr_ok); break;
-      default: break;
-    }
+// HS_K1_PINGPONG=1: uncontrolled dense gates write the second register array
+// (two-state interpreter); 0: every gate updates one array in place.
+#ifndef HS_K1_PINGPONG
+#define HS_K1_PINGPONG 0
+#endif
+
+template <bool FULL>
+__device__ __forceinline__ bool is_xfer(int code) {
+  return HS_K1_PINGPONG && (code < 4 || (FULL && code >= 64 && code < 70));
+}
+
+template <int R, bool FULL, typename V>
+__device__ __forceinline__ void op_xfer(const V (&s)[1 << R], V (&d)[1 << R], int code,
+                                        const double2* c) {
+#define X1(J) \
+  case (J): if constexpr ((J) < R) d1x<R, J>(s, d, c); break;
+#define X2(P, JA, JB) \
+  case 64 + (P): if constexpr (FULL && (JB) < R) d2x<R, JA, JB>(s, d, c); break;
+  switch (code) {
+    X1(0) X1(1) X1(2) X1(3)
+    X2(0, 0, 1) X2(1, 0, 2) X2(2, 0, 3) X2(3, 1, 2) X2(4, 1, 3) X2(5, 2, 3)
+    default: break;
   }
+#undef X1
+#undef X2
+}
+
+template <int R, bool FULL, typename V>
+__device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, const double2* c,
+                                           uint32_t thr, uint64_t gbase) {
+  // thread and outer part of the controls; register part is in the code / creg
+  const bool ok = ((thr & op.cthr) == op.cthr) && ((gbase & op.couter) == op.couter);
+  const uint32_t sm = ok ? 0x80000000u : 0u;
+  const double2 f = ok ? c[0] : make_double2(1.0, 0.0);
+#define C1(J) \
+  case 4 + (J): if constexpr ((J) < R) d1c<R, J>(v, c, op.creg, ok); break;
+#define NEG(M) \
+  case 16 + (M): if constexpr ((M) < (1 << R)) dneg<R, M>(v, sm); break;
+#define PH(M) \
+  case 32 + (M): if constexpr ((M) < (1 << R)) dphase<R, M>(v, f); break;
+#define C2(P, JA, JB) \
+  case 72 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, op.creg, ok); break;
+#define SW(P, JA, JB) \
+  case 80 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, true>(v, c, op.creg, ok); break;
+#define D1(J) \
+  case (J): if constexpr ((J) < R) d1c<R, J>(v, c, 0u, true); break;
+#define D2(P, JA, JB) \
+  case 64 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, 0u, true); break;
+  switch (op.code) {
+    D1(0) D1(1) D1(2) D1(3)
+    D2(0, 0, 1) D2(1, 0, 2) D2(2, 0, 3) D2(3, 1, 2) D2(4, 1, 3) D2(5, 2, 3)
+    C1(0) C1(1) C1(2) C1(3)
+    NEG(0) NEG(1) NEG(2) NEG(3) NEG(4) NEG(5) NEG(6) NEG(7)
+    NEG(8) NEG(9) NEG(10) NEG(11) NEG(12) NEG(13) NEG(14) NEG(15)
+    PH(0) PH(1) PH(2) PH(3) PH(4) PH(5) PH(6) PH(7)
+    PH(8) PH(9) PH(10) PH(11) PH(12) PH(13) PH(14) PH(15)
+    case 48: ddiag<R>(v, op, c, thr, gbase, ok); break;
+    C2(0, 0, 1) C2(1, 0, 2) C2(2, 0, 3) C2(3, 1, 2) C2(4, 1, 3) C2(5, 2, 3)
+    SW(0, 0, 1) SW(1, 0, 2) SW(2, 0, 3) SW(3, 1, 2) SW(4, 1, 3) SW(5, 2, 3)
+    default: break;
+  }
+#undef D1
+#undef D2
+#undef C1
+#undef NEG
+#undef PH
+#undef C2
+#undef SW
 }
 
 }  // namespace
 
 namespace {
 
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Shared-memory byte offset of tile index i: 16-byte slots hold 1 (complex128)
+// or 2 (complex64) amplitudes; slots are XOR-swizzled (swz is linear over
+// GF(2), so the offset of thr | reg(e) is built from per-bit parts).
+template <typename V>
+struct SmemMap {
+  static constexpr int SH = sizeof(V) == 8 ? 1 : 0;  // amplitudes per slot = 2^SH
+  __device__ __forceinline__ static uint32_t off(uint32_t i) {
+    return (swz(i >> SH) << 4) | ((i & ((1u << SH) - 1u)) * uint32_t(sizeof(V)));
+  }
+};
+
+// Issue the asynchronous copy of one tile into a shared buffer: 16-byte
+// chunks, chunk c covering tile indices [c*2^SH, (c+1)*2^SH) that are
+// contiguous in global memory (tile bit 0 is always global slot 0 when SH=1).
 template <int R, typename V>
-__global__ void __launch_bounds__(512, 1)
+__device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32_t sbuf,
+                                                uint64_t gbase, const uint64_t* __restrict__ gchunk,
+                                                uint64_t gt, int nchunk_per_thr) {
+  using M = SmemMap<V>;
+  const uint32_t t = threadIdx.x;
+  for (int k = 0; k < nchunk_per_thr; ++k) {
+    const uint32_t c = t + uint32_t(k) * blockDim.x;
+    const uint64_t g = gbase + gt + gchunk[k];
+    cp_async16(sbuf + (swz(c) << 4), sv + g);
+  }
+  (void)M::SH;
+}
+
+// tiles are at most 2^12 amplitudes (two buffers of 64 KiB for complex128):
+// 2^(12-R) = 256 threads
+template <typename V>
+struct K1Threads {
+  static constexpr int value = 256;
+};
+
+template <int R, bool FULL, typename V>
+__global__ void __launch_bounds__(K1Threads<V>::value, 1)
     k1_part(V* __restrict__ sv, const __grid_constant__ PartProgram P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* sm = reinterpret_cast<V*>(smem_raw);
+  using M = SmemMap<V>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int E = 1 << R;
   const uint32_t t = threadIdx.x;
-  V v[E];
+  const uint32_t nthr = blockDim.x;
+  const uint32_t tile_bytes = uint32_t(sizeof(V)) << P.m;
+  unsigned char* buf[2] = {smem_raw, smem_raw + tile_bytes};
+  uint64_t* s_gchunk = reinterpret_cast<uint64_t*>(smem_raw + 2 * tile_bytes);
+  // chunk c = t + k*nthr; its first tile index is c << SH.  The bits of t and
+  // of k*nthr are disjoint, so deposit(c << SH) = deposit(t << SH) + deposit(k*nthr << SH).
+  const int nchunk = (1 << P.m) >> M::SH;
+  const int per_thr = nchunk / int(nthr);
+  for (int k = t; k < per_thr; k += nthr)
+    s_gchunk[k] = deposit(uint64_t(k) * nthr << M::SH, P.tile);
+  __syncthreads();
+  const uint64_t gt = deposit(uint64_t(t) << M::SH, P.tile);
+  const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(buf[0]));
+  const uint32_t sb1 = uint32_t(__cvta_generic_to_shared(buf[1]));
 
-  // global offsets of this thread's elements for the first and the last group
-  const GroupDesc& g0 = P.groups[0];
-  const GroupDesc& gl = P.groups[P.ngroups - 1];
-  const uint64_t gthr0 = deposit(deposit(t, g0.thr), P.tile);
-  const uint64_t gthrl = deposit(deposit(t, gl.thr), P.tile);
-  uint64_t greg0[R], gregl[R];
-#pragma unroll
-  for (int j = 0; j < R; ++j) {
-    greg0[j] = deposit(1ull << g0.reg_tbit[j], P.tile);
-    gregl[j] = deposit(1ull << gl.reg_tbit[j], P.tile);
-  }
-
-  for (uint64_t tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
+  uint64_t tile = blockIdx.x;
+  if (tile < P.ntiles)
+    issue_tile_load<R, V>(sv, sb0, deposit(tile, P.outer), s_gchunk, gt, per_thr);
+  cp_async_commit();
+  V v[E], w[E];
+  for (int it = 0; tile < P.ntiles; ++it, tile += gridDim.x) {
+    const uint64_t next = tile + gridDim.x;
+    if (next < P.ntiles)
+      issue_tile_load<R, V>(sv, (it & 1) ? sb0 : sb1, deposit(next, P.outer), s_gchunk, gt,
+                            per_thr);
+    cp_async_commit();
+    cp_async_wait<1>();  // this tile's copies (all but the newest group) have landed
+    __syncthreads();
+    unsigned char* A = buf[it & 1];
     const uint64_t gbase = deposit(tile, P.outer);
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
       const uint32_t thr = uint32_t(deposit(t, G.thr));
-      if (g == 0) {
-        const V* src = sv + gbase + gthr0;
+      uint32_t sx[R], lo[R];  // per register bit: swizzled slot part / in-slot part
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          uint64_t off = 0;
-#pragma unroll
-          for (int j = 0; j < R; ++j)
-            if ((e >> j) & 1) off += greg0[j];
-          v[e] = __ldcs(src + off);
-        }
-      } else {
-        uint32_t rb[R];
-#pragma unroll
-        for (int j = 0; j < R; ++j) rb[j] = 1u << G.reg_tbit[j];
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-          uint32_t idx = thr;
-#pragma unroll
-          for (int j = 0; j < R; ++j)
-            if ((e >> j) & 1) idx |= rb[j];
-          v[e] = sm[swz(idx)];
-        }
-        __syncthreads();  // every read of this exchange precedes the next write
+      for (int j = 0; j < R; ++j) {
+        const uint32_t b = 1u << G.reg_tbit[j];
+        sx[j] = swz(b >> M::SH) << 4;
+        lo[j] = (b & ((1u << M::SH) - 1u)) * uint32_t(sizeof(V));
       }
-      for (int o = G.first_op; o < G.first_op + G.num_ops; ++o) {
-        const DevOp op = P.ops[o];
-        const bool thr_ok = ((thr & op.cthr) == op.cthr) && ((gbase & op.couter) == op.couter);
-        apply_op<R>(v, op, P.coef + op.coef, thr_ok);
+      const uint32_t sthr = M::off(thr);
+      uint32_t addr[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        uint32_t a = sthr;
+#pragma unroll
+        for (int j = 0; j < R; ++j)
+          if ((e >> j) & 1) a = (a ^ sx[j]) + lo[j];
+        addr[e] = a;
       }
-      if (g == P.ngroups - 1) {
-        V* dst = sv + gbase + gthrl;
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          uint64_t off = 0;
-#pragma unroll
-          for (int j = 0; j < R; ++j)
-            if ((e >> j) & 1) off += gregl[j];
-          __stcs(dst + off, v[e]);
+      for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(A + addr[e]);
+      // op descriptors and coefficients are read from the (warp-uniform)
+      // parameter space, so every dispatch below is a uniform branch
+      int o = G.first_op;
+      const int o_end = G.first_op + G.num_ops;
+    in_v:
+      while (o < o_end) {
+        const DevOp& op = P.ops[o++];
+        if (is_xfer<FULL>(op.code)) {
+          op_xfer<R, FULL>(v, w, op.code, P.coef + op.coef);
+          goto in_w;
         }
-      } else {
-        uint32_t rb[R];
-#pragma unroll
-        for (int j = 0; j < R; ++j) rb[j] = 1u << G.reg_tbit[j];
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-          uint32_t idx = thr;
-#pragma unroll
-          for (int j = 0; j < R; ++j)
-            if ((e >> j) & 1) idx |= rb[j];
-          sm[swz(idx)] = v[e];
-        }
-        __syncthreads();  // the whole tile is in shared memory
+        op_inplace<R, FULL>(v, op, P.coef + op.coef, thr, gbase);
       }
+#pragma unroll
+      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr[e]) = v[e];
+      goto group_done;
+    in_w:
+      while (o < o_end) {
+        const DevOp& op = P.ops[o++];
+        if (is_xfer<FULL>(op.code)) {
+          op_xfer<R, FULL>(w, v, op.code, P.coef + op.coef);
+          goto in_v;
+        }
+        op_inplace<R, FULL>(w, op, P.coef + op.coef, thr, gbase);
+      }
+#pragma unroll
+      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr[e]) = w[e];
+    group_done:
+      __syncthreads();  // the group's writes precede the next group's reads
     }
+    // write the tile back: chunk c = t + k*nthr, coalesced 16-byte stores
+    for (int k = 0; k < per_thr; ++k) {
+      const uint32_t c = t + uint32_t(k) * nthr;
+      const uint4 d = *reinterpret_cast<const uint4*>(A + (swz(c) << 4));
+      __stcs(reinterpret_cast<uint4*>(sv + gbase + gt + s_gchunk[k]), d);
+    }
+    __syncthreads();  // buffer A is free for the prefetch issued next iteration
   }
+  cp_async_wait<0>();
 }
 
 struct LaunchCfg {
@@ -274,50 +441,58 @@ struct LaunchCfg {
 
 int g_num_sms = 0;
 
-template <int R, typename V>
+template <int R, bool FULL, typename V>
 int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
   static bool attr_set[64] = {false};
   int dev = 0;
   HS_CUDA(cudaGetDevice(&dev));
   if (!attr_set[dev & 63]) {
-    HS_CUDA(cudaFuncSetAttribute(k1_part<R, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(V)) << kMaxTileBits));
+    HS_CUDA(cudaFuncSetAttribute(k1_part<R, FULL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 227 * 1024));
     attr_set[dev & 63] = true;
   }
   if (g_num_sms == 0) HS_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
   const int threads = 1 << (P.m - R);
-  const size_t smem = P.ngroups > 1 ? (sizeof(V) << P.m) : 0;
+  const int per_thr = ((1 << P.m) * int(sizeof(V)) / 16) / threads;
+  const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(uint64_t) * per_thr;
+  if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K1 tile of 2^%d needs %zu B", P.m, smem);
   int per_sm = 0;
-  HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, V>, threads, smem));
+  HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, V>, threads, smem));
   if (per_sm < 1) return set_error(HS_E_UNSUPPORTED, "K1 tile does not fit an SM (m=%d)", P.m);
   const uint64_t want = uint64_t(g_num_sms) * uint64_t(per_sm);
   const int grid = int(P.ntiles < want ? P.ntiles : want);
-  k1_part<R, V><<<grid, threads, smem, s>>>(sv, P);
+  k1_part<R, FULL, V><<<grid, threads, smem, s>>>(sv, P);
   HS_CUDA(cudaGetLastError());
   return HS_OK;
 }
 
 }  // namespace
 
-int launch_part(void* amp, int dtype, const PartProgram& P, cudaStream_t s) {
-  if (P.ngroups < 1 || P.nops < 1) return HS_OK;
+template <typename V>
+int launch_typed(V* a, const PartProgram& P, cudaStream_t s) {
+  bool full = false;
+  for (int i = 0; i < P.nops; ++i) full |= P.ops[i].kind == OP2_DENSE || P.ops[i].kind == OP2_SWAP;
   const int R = P.m < kRegBits ? P.m : kRegBits;
-  if (dtype == HS_DTYPE_C128) {
-    double2* a = static_cast<double2*>(amp);
+  if (full) {
     switch (R) {
-      case 1: return launch_k1<1>(a, P, s);
-      case 2: return launch_k1<2>(a, P, s);
-      case 3: return launch_k1<3>(a, P, s);
-      default: return launch_k1<4>(a, P, s);
+      case 1: return launch_k1<1, true>(a, P, s);
+      case 2: return launch_k1<2, true>(a, P, s);
+      case 3: return launch_k1<3, true>(a, P, s);
+      default: return launch_k1<4, true>(a, P, s);
     }
   }
-  float2* a = static_cast<float2*>(amp);
   switch (R) {
-    case 1: return launch_k1<1>(a, P, s);
-    case 2: return launch_k1<2>(a, P, s);
-    case 3: return launch_k1<3>(a, P, s);
-    default: return launch_k1<4>(a, P, s);
+    case 1: return launch_k1<1, false>(a, P, s);
+    case 2: return launch_k1<2, false>(a, P, s);
+    case 3: return launch_k1<3, false>(a, P, s);
+    default: return launch_k1<4, false>(a, P, s);
   }
+}
+
+int launch_part(void* amp, int dtype, const PartProgram& P, cudaStream_t s) {
+  if (P.ngroups < 1 || P.nops < 1) return HS_OK;
+  if (dtype == HS_DTYPE_C128) return launch_typed(static_cast<double2*>(amp), P, s);
+  return launch_typed(static_cast<float2*>(amp), P, s);
 }
 
 }  // namespace hisv

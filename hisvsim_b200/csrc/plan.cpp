@@ -7,11 +7,14 @@
 // is the same gather, widened by the lowest slots so that every global access
 // moves whole 32-byte sectors (the GPU form of opt_slots, execute.hpp:184-199).
 // Each tile is held by one CTA: 2^R amplitudes per thread in registers, where
-// R tile bits are "register bits"; a gate's targets must be register bits.
-// Consecutive gates whose targets fit in R bits form a group; between groups
-// the tile is exchanged through shared memory so that the next group's targets
-// become register bits.  Controls are predicates (register, thread or outer
-// bits), as control_offset is in StateVector::apply (state_vector.hpp:410-417).
+// R tile bits are "register bits".  A non-diagonal gate's targets must be
+// register bits; consecutive gates whose targets fit in R bits form a group,
+// and between groups the tile is exchanged through shared memory so that the
+// next group's targets become register bits.  Diagonal gates (Z, S, T, RZ,
+// controlled phases, RZZ, ...) only scale amplitudes by a phase chosen from
+// index bits, so they run in any layout and their qubits need not be in the
+// tile at all.  Controls are index predicates wherever their bits are, as
+// control_offset is in StateVector::apply (state_vector.hpp:410-417).
 #include <algorithm>
 #include <cstring>
 
@@ -38,48 +41,62 @@ void build_runs(const std::vector<int>& dst_of_src, Runs* r) {
 
 bool exact(cplx a, double re, double im = 0.0) { return a.real() == re && a.imag() == im; }
 
+bool is_diagonal(const LoweredGate& g) {
+  const int d = g.nt == 1 ? 2 : 4;
+  for (int r = 0; r < d; ++r)
+    for (int c = 0; c < d; ++c)
+      if (r != c && !exact(g.m[d * r + c], 0)) return false;
+  return true;
+}
+
 struct SlotGate {
   const LoweredGate* g;
-  int ts[2];   // target slots
+  bool diag;
+  int ts[2];  // target slots
   int nc;
   int cs[HS_MAX_CONTROLS];
 };
 
-int coef_count(const LoweredGate& g) {
-  const cplx* m = g.m;
-  if (g.nt == 1) {
-    if (exact(m[1], 0) && exact(m[2], 0)) {
-      if (exact(m[0], 1)) return exact(m[3], -1) ? 0 : 1;
-      return 2;
-    }
-    return 4;  // upper bound (X/H/Y use none)
-  }
-  bool diag = true;
-  for (int r = 0; r < 4; ++r)
-    for (int c = 0; c < 4; ++c)
-      if (r != c && !exact(m[4 * r + c], 0)) diag = false;
-  return diag ? 4 : 16;
+int coef_count(const SlotGate& sg) {
+  if (sg.diag) return 4;
+  return sg.g->nt == 1 ? 4 : 16;
 }
 
-// Fill the op for gate sg in group gd of a program whose tile maps slot ->
-// tile bit via tbit_of_slot (-1 outside the tile).
-void emit_op(const SlotGate& sg, const GroupDesc& gd, int R, const std::vector<int>& tbit_of_slot,
-             PartProgram* P) {
+struct Layout {
+  const std::vector<int>* tbit_of_slot;  // slot -> tile bit or -1
+  int regpos_of_tbit[kMaxTileBits];      // tile bit -> register position or -1
+};
+
+// where a slot's bit sits for the group: register / thread / outer
+void locate(const Layout& L, int slot, uint8_t* where, uint8_t* pos) {
+  const int tb = (*L.tbit_of_slot)[slot];
+  if (tb < 0) {
+    *where = TW_OUT;
+    *pos = uint8_t(slot);
+  } else if (L.regpos_of_tbit[tb] >= 0) {
+    *where = TW_REG;
+    *pos = uint8_t(L.regpos_of_tbit[tb]);
+  } else {
+    *where = TW_THR;
+    *pos = uint8_t(tb);
+  }
+}
+
+void add_mask_bit(const Layout& L, int slot, DevOp* op) {
+  uint8_t w, p;
+  locate(L, slot, &w, &p);
+  if (w == TW_OUT)
+    op->couter |= 1ull << p;
+  else if (w == TW_REG)
+    op->creg |= uint16_t(1u << p);
+  else
+    op->cthr |= 1u << p;
+}
+
+void emit_op(const SlotGate& sg, const Layout& L, PartProgram* P) {
   DevOp op;
   std::memset(&op, 0, sizeof(op));
-  int regpos_of_tbit[kMaxTileBits];
-  for (int b = 0; b < kMaxTileBits; ++b) regpos_of_tbit[b] = -1;
-  for (int j = 0; j < R; ++j) regpos_of_tbit[gd.reg_tbit[j]] = j;
-  for (int i = 0; i < sg.nc; ++i) {
-    int s = sg.cs[i];
-    int tb = tbit_of_slot[s];
-    if (tb < 0)
-      op.couter |= 1ull << s;
-    else if (regpos_of_tbit[tb] >= 0)
-      op.creg |= uint16_t(1u << regpos_of_tbit[tb]);
-    else
-      op.cthr |= 1u << tb;
-  }
+  for (int i = 0; i < sg.nc; ++i) add_mask_bit(L, sg.cs[i], &op);
   const cplx* m = sg.g->m;
   int base = P->ncoef;  // coefficients are appended in op order
   auto push = [&](cplx c) {
@@ -88,59 +105,75 @@ void emit_op(const SlotGate& sg, const GroupDesc& gd, int R, const std::vector<i
     ++base;
   };
   op.coef = uint16_t(base);
-  if (sg.g->nt == 1) {
-    op.ja = uint8_t(regpos_of_tbit[tbit_of_slot[sg.ts[0]]]);
-    const double s = 0.707106781186547524401;
-    if (exact(m[1], 0) && exact(m[2], 0)) {
-      if (exact(m[0], 1)) {
-        if (exact(m[3], -1)) {
-          op.kind = OP1_NEG;
-        } else {
-          op.kind = OP1_PHASE;
-          push(m[3]);
-        }
+  const bool ctrl = op.creg != 0 || op.cthr != 0 || op.couter != 0;
+  if (sg.diag) {
+    if (sg.g->nt == 1 && exact(m[0], 1)) {
+      // phase on the |1> of the target: a mask over controls + target
+      add_mask_bit(L, sg.ts[0], &op);
+      if (exact(m[3], -1)) {
+        op.kind = OPD_NEG;
       } else {
-        op.kind = OP1_DIAG;
-        push(m[0]);
+        op.kind = OPD_PHASE;
         push(m[3]);
       }
-    } else if (exact(m[0], 0) && exact(m[3], 0) && exact(m[1], 1) && exact(m[2], 1)) {
-      op.kind = OP1_X;
-    } else if (exact(m[0], s) && exact(m[1], s) && exact(m[2], s) && exact(m[3], -s)) {
-      op.kind = OP1_H;
-    } else if (exact(m[0], 0) && exact(m[3], 0) && exact(m[1], 0, -1) && exact(m[2], 0, 1)) {
-      op.kind = OP1_Y;
     } else {
-      op.kind = OP1_DENSE;
-      for (int k = 0; k < 4; ++k) push(m[k]);
+      op.kind = OPD_DIAG;
+      locate(L, sg.ts[0], &op.t0w, &op.t0p);
+      if (sg.g->nt == 1) {
+        push(m[0]);
+        push(m[3]);
+      } else {
+        // device index q = b(t0) | b(t1) << 1; reference index i = 2*b(t0) + b(t1)
+        locate(L, sg.ts[1], &op.t1w, &op.t1p);
+        push(m[0]);   // q=0: i=0
+        push(m[10]);  // q=1: b0=1,b1=0 -> i=2
+        push(m[5]);   // q=2: b0=0,b1=1 -> i=1
+        push(m[15]);  // q=3: i=3
+      }
     }
+    if (op.kind == OPD_NEG)
+      op.code = uint8_t(16 + op.creg);
+    else if (op.kind == OPD_PHASE)
+      op.code = uint8_t(32 + op.creg);
+    else
+      op.code = 48;
+  } else if (sg.g->nt == 1) {
+    uint8_t w;
+    locate(L, sg.ts[0], &w, &op.ja);
+    // every non-diagonal one-target gate runs as a dense 2x2 (X, Y and H
+    // included: multiplying by 0 and +-1 is exact, H differs from
+    // s*(a+b) by at most one rounding)
+    op.kind = OP1_DENSE;
+    for (int k = 0; k < 4; ++k) push(m[k]);
+    op.code = uint8_t((ctrl ? 4 : 0) + op.ja);
   } else {
-    int p0 = regpos_of_tbit[tbit_of_slot[sg.ts[0]]];
-    int p1 = regpos_of_tbit[tbit_of_slot[sg.ts[1]]];
-    op.ja = uint8_t(std::min(p0, p1));
-    op.jb = uint8_t(std::max(p0, p1));
+    uint8_t w;
+    uint8_t p0, p1;
+    locate(L, sg.ts[0], &w, &p0);
+    locate(L, sg.ts[1], &w, &p1);
+    op.ja = std::min(p0, p1);
+    op.jb = std::max(p0, p1);
     // device index q = b(ja) | b(jb) << 1; reference index i = 2*b(t0) + b(t1)
     auto ref_index = [&](int q) { return p0 < p1 ? (((q & 1) << 1) | (q >> 1)) : q; };
     cplx md[16];
     for (int qo = 0; qo < 4; ++qo)
       for (int qi = 0; qi < 4; ++qi) md[4 * qo + qi] = m[4 * ref_index(qo) + ref_index(qi)];
-    bool diag = true, swap = true;
+    bool swap = true;
     for (int r = 0; r < 4; ++r)
       for (int c = 0; c < 4; ++c) {
-        if (r != c && !exact(md[4 * r + c], 0)) diag = false;
         const bool one = (r == 0 && c == 0) || (r == 3 && c == 3) || (r == 1 && c == 2) ||
                          (r == 2 && c == 1);
         if (!exact(md[4 * r + c], one ? 1.0 : 0.0)) swap = false;
       }
     if (swap) {
       op.kind = OP2_SWAP;
-    } else if (diag) {
-      op.kind = OP2_DIAG;
-      for (int k = 0; k < 4; ++k) push(md[5 * k]);
     } else {
       op.kind = OP2_DENSE;
       for (int k = 0; k < 16; ++k) push(md[k]);
     }
+    static const int pair_index[4][4] = {{-1, 0, 1, 2}, {-1, -1, 3, 4}, {-1, -1, -1, 5},
+                                         {-1, -1, -1, -1}};
+    op.code = uint8_t((op.kind == OP2_SWAP ? 80 : (ctrl ? 72 : 64)) + pair_index[op.ja][op.jb]);
   }
   P->ncoef = base;
   P->ops[P->nops++] = op;
@@ -149,41 +182,46 @@ void emit_op(const SlotGate& sg, const GroupDesc& gd, int R, const std::vector<i
 }  // namespace
 
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
-              int tile_bits_hint, std::vector<PartProgram>* programs) {
+              int tile_bits_hint, int dtype, std::vector<PartProgram>* programs) {
   programs->clear();
   if (n < 1 || n > 63) return set_error(HS_E_INVALID, "bad qubit count %d", n);
-  const int max_tile = std::min(n, kMaxTileBits);
-  const int m_target = std::min(n, tile_bits_hint > 0 ? std::min(tile_bits_hint, kMaxTileBits)
-                                                      : 12);
-  const int low_min = std::min(n, 3);
+  // two tile buffers must fit in shared memory: 2^12 complex128 / 2^13 complex64
+  const int max_tile = std::min(n, max_tile_bits(dtype));
+  const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : max_tile);
+  // keep the lowest slots in the tile so that global accesses come in
+  // contiguous runs of at least 64 bytes (complex64 tiles also need slot 0 for
+  // their 16-byte chunks)
+  const int low_min = std::min(n, dtype == HS_DTYPE_C64 ? 3 : 2);
   std::vector<SlotGate> sgs;
   for (const auto& g : gates) {
     if (g.nt == 0) continue;
     SlotGate s;
     s.g = &g;
+    s.diag = is_diagonal(g);
     for (int i = 0; i < g.nt; ++i) s.ts[i] = q2s[g.targets[i]];
     s.nc = g.nc;
     for (int i = 0; i < g.nc; ++i) s.cs[i] = q2s[g.controls[i]];
     sgs.push_back(s);
   }
+  auto low_union_size = [&](const std::vector<int>& t) {
+    int extra = 0;
+    for (int s = 0; s < low_min; ++s)
+      if (std::find(t.begin(), t.end(), s) == t.end()) ++extra;
+    return int(t.size()) + extra;
+  };
   size_t gi = 0;
   while (gi < sgs.size()) {
-    // ---- chunk: gates whose target slots (plus the low slots) fit one tile
-    std::vector<int> tset;  // target slots in the chunk
-    auto low_union_size = [&](const std::vector<int>& t) {
-      int extra = 0;
-      for (int s = 0; s < low_min; ++s)
-        if (std::find(t.begin(), t.end(), s) == t.end()) ++extra;
-      return int(t.size()) + extra;
-    };
+    // ---- chunk: gates whose non-diagonal target slots (+ low slots) fit one tile
+    std::vector<int> tset;
     size_t gend = gi;
     int ops = 0, coefs = 0;
     while (gend < sgs.size()) {
       std::vector<int> t2 = tset;
-      for (int i = 0; i < sgs[gend].g->nt; ++i)
-        if (std::find(t2.begin(), t2.end(), sgs[gend].ts[i]) == t2.end())
-          t2.push_back(sgs[gend].ts[i]);
-      const int cc = coef_count(*sgs[gend].g);
+      if (!sgs[gend].diag)
+        for (int i = 0; i < sgs[gend].g->nt; ++i)
+          if (std::find(t2.begin(), t2.end(), sgs[gend].ts[i]) == t2.end())
+            t2.push_back(sgs[gend].ts[i]);
+      const int cc = coef_count(sgs[gend]);
       if (low_union_size(t2) > max_tile || ops + 1 > kMaxOps || coefs + cc > kMaxCoef) break;
       tset = t2;
       ++ops;
@@ -191,18 +229,16 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       ++gend;
     }
     if (gend == gi) return set_error(HS_E_INVALID, "gate does not fit a tile");
-    // ---- tile: target slots + lowest slots up to the target size
+    // ---- tile: non-diagonal target slots + lowest slots up to the target size
     std::vector<int> tile = tset;
-    const int m = std::max(m_target, low_union_size(tset));
+    const int m = std::min(max_tile, std::max(m_target, low_union_size(tset)));
     for (int s = 0; s < n && int(tile.size()) < m; ++s)
       if (std::find(tile.begin(), tile.end(), s) == tile.end()) tile.push_back(s);
     std::sort(tile.begin(), tile.end());
     const int R = std::min(kRegBits, m);
     std::vector<int> tbit_of_slot(n, -1);
     for (int i = 0; i < m; ++i) tbit_of_slot[tile[i]] = i;
-    // ---- groups over [gi, gend)
     PartProgram* P = nullptr;
-    size_t k = gi;
     auto new_program = [&]() {
       programs->emplace_back();
       P = &programs->back();
@@ -211,24 +247,55 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       P->m = m;
       P->ntiles = 1ull << (n - m);
       build_runs(tile, &P->tile);
+      for (int b = 0; b < m; ++b) P->tile_slot[b] = uint8_t(tile[b]);
       std::vector<int> outer;
       for (int s = 0; s < n; ++s)
         if (tbit_of_slot[s] < 0) outer.push_back(s);
       build_runs(outer, &P->outer);
     };
     new_program();
-    while (k < gend) {
-      std::vector<int> regs;  // tile bits needed in registers
-      size_t e = k;
-      while (e < gend) {
-        std::vector<int> r2 = regs;
-        for (int i = 0; i < sgs[e].g->nt; ++i) {
-          int tb = tbit_of_slot[sgs[e].ts[i]];
-          if (std::find(r2.begin(), r2.end(), tb) == r2.end()) r2.push_back(tb);
+    // ---- groups: a second-level acyclic partition of the chunk.  Each group
+    // takes, in circuit order, every remaining gate whose non-diagonal targets
+    // fit the R register bits and none of whose qubits is held by a gate left
+    // for a later group (so every gate still follows all gates it depends on).
+    std::vector<size_t> remaining;
+    for (size_t x = gi; x < gend; ++x) remaining.push_back(x);
+    while (!remaining.empty()) {
+      std::vector<int> regs;
+      std::vector<size_t> members, rest;
+      std::vector<int> blocked;  // slots held back by a deferred gate
+      auto touches = [&](const SlotGate& g, const std::vector<int>& set) {
+        for (int i = 0; i < g.g->nt; ++i)
+          if (std::find(set.begin(), set.end(), g.ts[i]) != set.end()) return true;
+        for (int i = 0; i < g.nc; ++i)
+          if (std::find(set.begin(), set.end(), g.cs[i]) != set.end()) return true;
+        return false;
+      };
+      auto block = [&](const SlotGate& g) {
+        for (int i = 0; i < g.g->nt; ++i) blocked.push_back(g.ts[i]);
+        for (int i = 0; i < g.nc; ++i) blocked.push_back(g.cs[i]);
+      };
+      for (size_t x : remaining) {
+        const SlotGate& g = sgs[x];
+        if (touches(g, blocked)) {
+          block(g);
+          rest.push_back(x);
+          continue;
         }
-        if (int(r2.size()) > R) break;
-        regs = r2;
-        ++e;
+        if (!g.diag) {
+          std::vector<int> r2 = regs;
+          for (int i = 0; i < g.g->nt; ++i) {
+            const int tb = tbit_of_slot[g.ts[i]];
+            if (std::find(r2.begin(), r2.end(), tb) == r2.end()) r2.push_back(tb);
+          }
+          if (int(r2.size()) > R) {
+            block(g);
+            rest.push_back(x);
+            continue;
+          }
+          regs = r2;
+        }
+        members.push_back(x);
       }
       if (P->ngroups == kMaxGroups) new_program();  // a new pass (rare)
       GroupDesc& gd = P->groups[P->ngroups++];
@@ -243,10 +310,14 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       for (int b = 0; b < m; ++b)
         if (std::find(regs.begin(), regs.end(), b) == regs.end()) thr.push_back(b);
       build_runs(thr, &gd.thr);
+      Layout L;
+      L.tbit_of_slot = &tbit_of_slot;
+      for (int b = 0; b < kMaxTileBits; ++b) L.regpos_of_tbit[b] = -1;
+      for (int j = 0; j < R; ++j) L.regpos_of_tbit[regs[j]] = j;
       gd.first_op = uint16_t(P->nops);
-      for (size_t x = k; x < e; ++x) emit_op(sgs[x], gd, R, tbit_of_slot, P);
+      for (size_t x : members) emit_op(sgs[x], L, P);
       gd.num_ops = uint16_t(P->nops - gd.first_op);
-      k = e;
+      remaining = rest;
     }
     gi = gend;
   }

@@ -166,6 +166,12 @@ int hs_part_run(hs_state* st, const hs_gate* gates, int num_gates, void* stream)
 int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
                  int num_parts, void* stream);
 
+/* Host-only: plan one part (identity slot map) without touching a device and
+ * report stats[0..5] = {passes, register groups, ops, dense ops, diagonal
+ * ops, tile bits}.  Used by the cost model and by tests of the planner. */
+int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates,
+                  int32_t* stats);
+
 /* Tile-size override for K1 (0 = automatic).  Returns the previous value. */
 int hs_set_tile_qubits(int m);
 
