@@ -67,6 +67,7 @@ SIGNATURES = {
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
+    "hs_norm2_noalloc": [_vp, _dp, _vp],
     "hs_inner": [_vp, _vp, _dp],
     "hs_max_abs_diff": [_vp, _vp, _dp],
     "hs_probability": [_vp, _i, _i, _dp],

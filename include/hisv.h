@@ -197,6 +197,16 @@ int hs_norm2(hs_state* st, double* out);
 int hs_inner(hs_state* a, hs_state* b, double out[2]);
 /* max_i |a_i - b_i| (state_equal / operator==, state_vector.hpp:1003-1072). */
 int hs_max_abs_diff(hs_state* a, hs_state* b, double* out);
+/* sum |a|^2 like hs_norm2, but allocating no device memory (no counterpart in
+ * the reference).  For callers that may not let the library call cudaMalloc /
+ * cudaFree: hosts that give all device memory to their own pool, or loops that
+ * must not incur the synchronisation those calls can cause.  Partial sums live
+ * in a fixed 1 MiB array in the library's device image, so states of at most
+ * 2^33 amplitudes are accepted (HS_E_UNSUPPORTED beyond).  The first call on a
+ * device looks the array's address up (make it before any stream capture);
+ * calls share the array, so calls that overlap on the GPU race.  Synchronises
+ * `stream` before returning. */
+int hs_norm2_noalloc(hs_state* st, double* out, void* stream);
 /* probability(qubit, value) (state_vector.hpp:897-923), race-free. */
 int hs_probability(hs_state* st, int qubit, int value, double* out);
 /* <Z_i Z_j> for num_pairs qubit pairs. */
