@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--tile-qubits", type=int, default=11, help="K1 tile bits (0 = automatic)")
+    ap.add_argument("--no-fused", action="store_true", help="skip the precision form")
+    ap.add_argument("--no-fidelity", action="store_true", help="skip the 1-F check")
     return ap.parse_args()
 
 
@@ -198,12 +200,36 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def timed_steps(abi, step, warmup, steps, pg, device):
+    """W untimed steps, then K steps between events on the library stream."""
+    for _ in range(warmup):
+        step()
+    abi.synchronize()
+    abi.counters_reset()
+    abi.set_timing(True)
+    barrier(pg)
+    start, stop = abi.Event(), abi.Event()
+    with ClockSampler(device) as clk:
+        abi.synchronize()
+        start.record()
+        for _ in range(steps):
+            step()
+        stop.record()
+        ms = start.elapsed_ms(stop)
+    abi.set_timing(False)
+    c = abi.counters()
+    return dist_max(pg, ms / 1e3 / steps), c, clk.summary()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference_arm(args)
     rank, world, local, pg = dist_setup(args.gpus)
-    from hisvsim_b200 import abi
+    import numpy as np
+
+    from hisvsim_b200 import abi, partition
+    from hisvsim_b200.gates import part_offsets
 
     abi.set_device(local)
     if args.tile_qubits:
@@ -211,55 +237,79 @@ def main():
     n = args.qubits
     gates, parts, rec, offs = workload(n, args.layers, args.seed + rank, args.part_qubits)
     upd = len(gates) * float(1 << n)
-
-    st = abi.State(n, abi.C128)
-    start, stop = abi.Event(), abi.Event()
-
-    def step():
-        st.set_basis(0)
-        st.run_parts(rec, offs)
-
-    for _ in range(args.warmup):
-        step()
-    abi.synchronize()
-    abi.counters_reset()
-    abi.set_timing(True)
-    barrier(pg)
-    with ClockSampler(local) as clk:
-        abi.synchronize()
-        start.record()
-        for _ in range(args.steps):
-            step()
-        stop.record()
-        ms = start.elapsed_ms(stop)
-    abi.set_timing(False)
-    c = abi.counters()
-    pbytes = abi.launch_bytes()
-    t_step = dist_max(pg, ms / 1e3 / args.steps)
-    passes = c["passes"] / args.steps
-    k1_avg_ms = c["apply_us"] / 1e3 / max(1, c["passes"])
-    bytes_per_pass = 2.0 * (1 << n) * 16
-    norm = st.norm2()
-
-    peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak_gbs, peak_src = float(peaks["hbm_gbs"]), "measured"
     except Exception:
         peak_gbs, peak_src = 6650.0, "fallback"
+
+    # ---- precision form: complex64 state, one 64x64 unitary per part of <= 6
+    # qubits, split-BF16 tensor-core GEMMs (timed first; its result is kept in
+    # host memory for the fidelity check against the complex128 run)
+    fused = None
+    fused_host = None
+    if not args.no_fused:
+        fparts = partition.partition_acyclic(gates, 6)
+        frec, foffs = part_offsets(partition.parts_to_gates(gates, fparts))
+        stf = abi.State(n, abi.C64)
+
+        def fstep():
+            stf.set_basis(0)
+            stf.run_fused(frec, foffs, 0)
+
+        t_f, cf, clk_f = timed_steps(abi, fstep, args.warmup, args.steps, pg, local)
+        fpasses = cf["passes"] / args.steps
+        fbytes = 2.0 * (1 << n) * 8
+        k4_ms = cf["apply_us"] / 1e3 / max(1, cf["passes"])
+        fused = {"circuit_s": t_f, "parts": len(fparts), "passes_per_step": fpasses,
+                 "value": world * upd / t_f, "unit": UNIT,
+                 "hbm_GBps": fpasses * fbytes / t_f / 1e9,
+                 "roofline": {"bound": "hbm", "kernel": "k4_fused", "avg_launch_ms": k4_ms,
+                              "achieved": fbytes / (k4_ms / 1e3) / 1e9 if k4_ms else None,
+                              "peak": peak_gbs, "unit": "GB/s",
+                              "frac": fbytes / (k4_ms / 1e3) / 1e9 / peak_gbs if k4_ms else None},
+                 "dtype": "c64 state, bf16x3 split operands, fp32 accumulate, fp64 unitaries",
+                 "clocks": clk_f}
+        if rank == 0 and not args.no_fidelity:
+            fused_host = stf.raw()
+        stf.close()
+        del stf
+
+    # ---- plain form (the drop-in): complex128, K1 passes
+    st = abi.State(n, abi.C128)
+
+    def step():
+        st.set_basis(0)
+        st.run_parts(rec, offs)
+
+    t_step, c, clk = timed_steps(abi, step, args.warmup, args.steps, pg, local)
+    pbytes = abi.launch_bytes()
+    passes = c["passes"] / args.steps
+    k1_avg_ms = c["apply_us"] / 1e3 / max(1, c["passes"])
+    bytes_per_pass = 2.0 * (1 << n) * 16
+    norm = st.norm2()
     k1_gbs = bytes_per_pass / (k1_avg_ms / 1e3) / 1e9
+    if fused is not None:
+        fused["speedup_vs_plain"] = t_step / fused["circuit_s"]
+        if fused_host is not None:
+            cmpd = st.compare_host(fused_host)
+            fused["fidelity_loss"] = 1.0 - cmpd["fidelity"]
+            fused["max_abs_err"] = cmpd["max_abs_diff"]
+            fused["fidelity_ref"] = f"complex128 plain run of the same {n}-qubit circuit"
+            del fused_host
     traffic = None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "k1_traffic.json")))
-        traffic = tr.get("bytes_per_launch_scaled_33q")
+        traffic = tr.get("bytes_per_launch_scaled")
     except Exception:
         pass
+    st.close()
+    del st
 
     # end to end through the public API (pybind module): allocate, run every
     # part from host gate lists, read back the norm
     e2e = None
     if not args.no_e2e:
-        del st
         from hisvsim_b200 import svsimulator_py_wrapper as svsim
         from hisvsim_b200.gates import NOPARAM
 
@@ -272,22 +322,23 @@ def main():
                                    list(g.targets))
 
         lists = [[bound(gates[i]) for i in p] for p in parts]
+        e2e_steps = max(1, min(args.steps, 2))
         abi.counters_reset()
         barrier(pg)
         t0 = time.perf_counter()
-        for _ in range(max(1, min(args.steps, 2))):
+        for _ in range(e2e_steps):
             sim = svsim.StateVector(n, 0)
             for bl in lists:
                 svsim.gather_and_execute_on(sim, bl)
             _ = sim.norm()
             del sim
-        e2e_steps = max(1, min(args.steps, 2))
         t_e2e = dist_max(pg, (time.perf_counter() - t0) / e2e_steps)
         e2e = {"value": world * upd / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": abi.launch_bytes() // e2e_steps,
                "d2h_bytes_per_step": 16, "circuit_s": t_e2e,
                "path": "svsimulator_py_wrapper: StateVector -> gather_and_execute_on per part "
-                       "-> norm readback"}
+                       "-> norm readback (gate programs travel as kernel parameters; the "
+                       "initial state |0..0> is created on the device, as StateVector does)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -306,9 +357,9 @@ def main():
             "config": {"workload": f"random circuit {n} qubits x {args.layers} layers "
                                    f"(U3 all qubits + CZ random matching), plain complex128",
                        "gates": len(gates), "parts": len(parts),
-                       "part_qubits": args.part_qubits, "passes_per_step": passes,
-                       "state_bytes": (1 << n) * 16, "l2": "state 128 GiB >> L2, no flush",
-                       "parallelism": f"replicas{world}"},
+                       "part_qubits": args.part_qubits, "tile_qubits": args.tile_qubits,
+                       "passes_per_step": passes, "state_bytes": (1 << n) * 16,
+                       "l2": "state >> L2 (126 MB), no flush", "parallelism": f"replicas{world}"},
             "circuit_s": t_step, "hbm_GBps": passes * bytes_per_pass / t_step / 1e9,
             "hbm_frac": passes * bytes_per_pass / t_step / 1e9 / peak_gbs,
             "norm": norm,
@@ -316,9 +367,10 @@ def main():
                          "frac": k1_gbs / peak_gbs, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "k1_part", "algorithmic_bytes_per_launch": bytes_per_pass,
                          "avg_launch_ms": k1_avg_ms},
+            "fused": fused,
             "gpu_launches": int(c["passes"] + args.steps),
             "launch_param_bytes_per_step": pbytes / args.steps,
-            "clocks": clk.summary(),
+            "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
         }

@@ -64,6 +64,10 @@ SIGNATURES = {
     "hs_parts_run": [_vp, _vp, _vp, _i, _vp],
     "hs_set_tile_qubits": [_i],
     "hs_plan_stats": [_i, _i, _vp, _i, _vp],
+    "hs_fused_parts_run": [_vp, _vp, _vp, _i, _i, _vp],
+    "hs_fused_compose": [_i, _vp, _vp, _i, _vp, _vp],
+    "hs_compare": [_vp, _vp, _dp],
+    "hs_compare_host": [_vp, _vp, _i, _dp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
@@ -191,6 +195,34 @@ class State:
         offsets = np.ascontiguousarray(offsets, dtype=np.int32)
         check(lib().hs_parts_run(self.h, _ptr(records), _ptr(offsets), len(offsets) - 1, stream))
 
+    def run_fused(self, records: np.ndarray, offsets: np.ndarray, precision: int = 0,
+                  stream=None):
+        """Precision form: one fused unitary per part, tensor-core GEMMs (complex64)."""
+        records = _records(records)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        check(lib().hs_fused_parts_run(self.h, _ptr(records), _ptr(offsets), len(offsets) - 1,
+                                       precision, stream))
+
+    def compare(self, other: "State") -> dict:
+        """<self|other>, max |self - other|, <other|other> and the fidelity."""
+        out = np.zeros(4)
+        check(lib().hs_compare(self.h, other.h, out.ctypes.data_as(_dp)))
+        ip = complex(out[0], out[1])
+        na = self.norm2()
+        return {"inner": ip, "max_abs_diff": out[2], "norm_other": out[3],
+                "fidelity": abs(ip) ** 2 / (na * out[3]) if na * out[3] > 0 else 0.0}
+
+    def compare_host(self, host: np.ndarray) -> dict:
+        """compare() against amplitudes held in host memory (qubit order)."""
+        host = np.ascontiguousarray(host)
+        dt = C128 if host.dtype == np.complex128 else C64
+        out = np.zeros(4)
+        check(lib().hs_compare_host(self.h, _ptr(host), dt, out.ctypes.data_as(_dp)))
+        ip = complex(out[0], out[1])
+        na = self.norm2()
+        return {"inner": ip, "max_abs_diff": out[2], "norm_other": out[3],
+                "fidelity": abs(ip) ** 2 / (na * out[3]) if na * out[3] > 0 else 0.0}
+
     def permute_bits(self, pairs: Sequence[int], stream=None):
         p = np.ascontiguousarray(pairs, dtype=np.int32).reshape(-1)
         check(lib().hs_permute_bits(self.h, _ptr(p), len(p) // 2, stream))
@@ -239,6 +271,17 @@ def plan_stats(n: int, gates, dtype: int = C128) -> dict:
     out = np.zeros(6, dtype=np.int32)
     check(lib().hs_plan_stats(n, dtype, _ptr(rec), len(rec), _ptr(out)))
     return dict(zip(["passes", "groups", "ops", "dense", "diag", "tile_bits"], out.tolist()))
+
+
+def fused_compose(n: int, records: np.ndarray, offsets: np.ndarray):
+    """K5 only: FP64 unitaries (parts x 64 x 64) and the qubit of each local bit."""
+    records = _records(records)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    nparts = len(offsets) - 1
+    u = np.zeros((nparts, 64, 64), dtype=np.complex128)
+    q = np.zeros((nparts, 6), dtype=np.int32)
+    check(lib().hs_fused_compose(n, _ptr(records), _ptr(offsets), nparts, _ptr(u), _ptr(q)))
+    return u, q
 
 
 def set_device(d: int):

@@ -37,6 +37,22 @@ void count_pass(long long gates) {
   g_gates += gates;
 }
 
+TimedRegion::TimedRegion(cudaStream_t s_) : s(s_) {
+  if (g_timing.load()) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+  }
+}
+
+TimedRegion::~TimedRegion() {
+  if (a) {
+    cudaEventRecord(b, s);
+    std::lock_guard<std::mutex> lk(g_ev_mu);
+    g_events.emplace_back(a, b);
+  }
+}
+
 namespace {
 
 cudaStream_t S(void* stream) { return static_cast<cudaStream_t>(stream); }
@@ -45,25 +61,6 @@ int check_state(const hs_state* st) {
   if (!st || !st->amp) return set_error(HS_E_INVALID, "null or destroyed state");
   return HS_OK;
 }
-
-struct TimedRegion {
-  cudaStream_t s;
-  cudaEvent_t a = nullptr, b = nullptr;
-  explicit TimedRegion(cudaStream_t s_) : s(s_) {
-    if (g_timing.load()) {
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      cudaEventRecord(a, s);
-    }
-  }
-  ~TimedRegion() {
-    if (a) {
-      cudaEventRecord(b, s);
-      std::lock_guard<std::mutex> lk(g_ev_mu);
-      g_events.emplace_back(a, b);
-    }
-  }
-};
 
 // Apply a permutation of bit positions to the data: the bit at position p
 // moves to position pi[p].  Done as two in-place involution passes of K2:

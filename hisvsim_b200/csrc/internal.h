@@ -140,6 +140,38 @@ struct PermProgram {
   uint8_t hha[32], hhb[32];
 };
 
+// ---- precision form: fused 64x64 unitaries (kernels_fused.cu) ----------------
+constexpr int kFusedBits = 6;   // qubits per fused unitary
+constexpr int kFusedDim = 64;
+constexpr int kFusedMaxOps = 2;  // fused unitaries applied per state pass
+constexpr int kFusedABytes = 2 * 128 * 128 * 2;  // BF16 hi + lo of the real 128x128 form
+
+// one gate of a part in the part's local bits (local bit j = j-th lowest slot)
+struct FusedGate {
+  int32_t nt;         // 1 or 2
+  int32_t t0, t1;     // local target bits
+  int32_t cmask;      // local control bits
+  double2 m[16];      // 2x2 (m[0..3]) or 4x4, reference index i = 2*b(t0) + b(t1)
+};
+
+struct FusedPass {
+  int32_t n, m;
+  uint64_t ntiles;
+  Runs tile, outer;
+  int32_t nops;
+  int32_t precision;                // 0: 3 BF16 products, 1: one product
+  int32_t part[kFusedMaxOps];       // index of the part's A operand
+  uint8_t pbits[kFusedMaxOps][kFusedBits];  // tile bit of local bit j
+};
+
+int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, double2* d_u,
+                   void* d_a, cudaStream_t s);
+int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cudaStream_t s);
+int reduce_compare(const void* a, int adtype, const void* b, int bdtype, int n, double out[4],
+                   cudaStream_t s);
+int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, uint64_t count,
+                         double out[4], cudaStream_t s);
+
 // ---- launchers (kernels_*.cu) ----------------------------------------------
 int launch_part(void* amp, int dtype, const PartProgram& prog, cudaStream_t s);
 int launch_permute(void* amp, int dtype, int n, const int32_t* pairs, int npairs,
@@ -160,6 +192,13 @@ int convert_kernel(const void* src, int sdtype, void* dst, int ddtype, uint64_t 
 
 // ---- counters ---------------------------------------------------------------
 void count_pass(long long gates);
+// device-time accounting (hs_set_timing): brackets launches with CUDA events
+struct TimedRegion {
+  cudaStream_t s;
+  cudaEvent_t a = nullptr, b = nullptr;
+  explicit TimedRegion(cudaStream_t s_);
+  ~TimedRegion();
+};
 
 inline size_t amp_bytes(int dtype) { return dtype == HS_DTYPE_C64 ? 8 : 16; }
 

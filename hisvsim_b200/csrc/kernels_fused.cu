@@ -1,0 +1,321 @@
+// Precision form: each part (<= 6 qubits) is fused into a 64x64 complex
+// unitary composed in FP64 (K5) and applied to a complex64 state on the
+// tcgen05 tensor cores (K4) as a real GEMM with split-BF16 operands and FP32
+// accumulation.
+//
+// Complex product Y = U X as one real product with (re, im) interleaved:
+//     Y[2p + c] = sum_k A[2p + c][k] X[k],  A[2po+co][2pi+ci] = the 2x2 real
+//     block [[Re, -Im], [Im, Re]] of U(po, pi)   (A: 128 x 128, B: 128 x N)
+// with X the tile viewed as 64 (part index) x N (other tile bits).  Each FP32
+// operand x is split as hi = bf16(x), lo = bf16(x - hi) and the product is
+// Ah*Bh + Ah*Bl + Al*Bh (the Al*Bl term, ~2^-16 relative, is dropped).
+#include <cuda_bf16.h>
+
+#include "internal.h"
+#include "tcgen05.cuh"
+
+namespace hisv {
+namespace {
+
+// ---- K5: compose each part's unitary in FP64 --------------------------------
+// One CTA per part, thread j owns column j of U (the image of basis state j);
+// U lives row-major in shared memory so that a warp's accesses are contiguous.
+__global__ void __launch_bounds__(64) k5_compose(const FusedGate* __restrict__ gates,
+                                                 const int32_t* __restrict__ offs,
+                                                 double2* __restrict__ u_out,
+                                                 uint8_t* __restrict__ a_out) {
+  extern __shared__ __align__(16) double2 U[];  // [64][64]
+  const int part = blockIdx.x;
+  const int j = threadIdx.x;
+  for (int i = 0; i < kFusedDim; ++i) U[i * kFusedDim + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  for (int g = offs[part]; g < offs[part + 1]; ++g) {
+    const FusedGate& G = gates[g];
+    if (G.nt == 1) {
+      const int t = 1 << G.t0;
+      for (int i = 0; i < kFusedDim; ++i) {
+        if ((i & t) || (i & G.cmask) != G.cmask) continue;
+        const double2 a = U[i * kFusedDim + j], b = U[(i | t) * kFusedDim + j];
+        const double2 m0 = G.m[0], m1 = G.m[1], m2 = G.m[2], m3 = G.m[3];
+        U[i * kFusedDim + j] = make_double2(m0.x * a.x - m0.y * a.y + m1.x * b.x - m1.y * b.y,
+                                            m0.x * a.y + m0.y * a.x + m1.x * b.y + m1.y * b.x);
+        U[(i | t) * kFusedDim + j] =
+            make_double2(m2.x * a.x - m2.y * a.y + m3.x * b.x - m3.y * b.y,
+                         m2.x * a.y + m2.y * a.x + m3.x * b.y + m3.y * b.x);
+      }
+    } else {
+      const int b0 = 1 << G.t0, b1 = 1 << G.t1;
+      for (int i = 0; i < kFusedDim; ++i) {
+        if ((i & (b0 | b1)) || (i & G.cmask) != G.cmask) continue;
+        const int idx[4] = {i, i | b1, i | b0, i | b0 | b1};  // reference index 2*b(t0)+b(t1)
+        double2 in[4];
+        for (int q = 0; q < 4; ++q) in[q] = U[idx[q] * kFusedDim + j];
+        for (int r = 0; r < 4; ++r) {
+          double re = 0, im = 0;
+          for (int q = 0; q < 4; ++q) {
+            const double2 c = G.m[4 * r + q];
+            re += c.x * in[q].x - c.y * in[q].y;
+            im += c.x * in[q].y + c.y * in[q].x;
+          }
+          U[idx[r] * kFusedDim + j] = make_double2(re, im);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (u_out) {
+    double2* uo = u_out + size_t(part) * kFusedDim * kFusedDim;
+    for (int i = 0; i < kFusedDim; ++i) uo[i * kFusedDim + j] = U[i * kFusedDim + j];
+  }
+  // The real form with (re, im) interleaved: row r = 2*po + co, column
+  // k = 2*pi + ci holds Re U (co = ci), -Im U (co=0, ci=1) or Im U (co=1, ci=0)
+  // of U(po, pi); stored as BF16 hi / lo in the K-major operand layout.
+  uint8_t* ao = a_out + size_t(part) * kFusedABytes;
+  for (int e = j; e < 128 * 128; e += kFusedDim) {
+    const int r = e >> 7, c = e & 127;
+    const double2 u = U[(r >> 1) * kFusedDim + (c >> 1)];
+    const int co = r & 1, ci = c & 1;
+    const double x = co == ci ? u.x : (co == 0 ? -u.y : u.y);
+    const __nv_bfloat16 hi = __double2bfloat16(x);
+    const __nv_bfloat16 lo = __double2bfloat16(x - double(__bfloat162float(hi)));
+    const uint32_t off = tc::kmajor_off(uint32_t(r), uint32_t(c), 2048u);
+    *reinterpret_cast<__nv_bfloat16*>(ao + off) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(ao + kFusedABytes / 2 + off) = lo;
+  }
+}
+
+// ---- K4: apply fused unitaries to complex64 tiles on the tensor cores --------
+constexpr int kK4Threads = 256;
+constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before giving up
+
+__device__ __forceinline__ uint64_t dep(uint64_t x, const Runs& r) {
+  uint64_t out = 0;
+  for (int i = 0; i < r.n; ++i) out |= ((x >> r.src[i]) & ((1ull << r.len[i]) - 1ull)) << r.dst[i];
+  return out;
+}
+
+// tile buffer position of tile index i: bits 1..3 XOR a fold of bits >= 4, so
+// that accesses spread over the banks; bit 0 is kept so that the two
+// amplitudes of a 16-byte chunk stay adjacent
+__device__ __forceinline__ uint32_t tswz(uint32_t i) {
+  return i ^ ((((i >> 4) ^ (i >> 7) ^ (i >> 10)) & 7u) << 1);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Shared memory: [A: nops x 64 KiB][B hi | B lo: N x 256 B each]
+//                [tile buffers: 2 x 2^m complex64][tables][mbarrier][TMEM address]
+// The next tile streams into the second buffer (cp.async, 16-byte chunks of two
+// amplitudes) while the current one is processed.
+__global__ void __launch_bounds__(kK4Threads, 1)
+    k4_fused(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
+             const uint8_t* __restrict__ a_all, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m = P.m;
+  const int T = 1 << m;            // tile amplitudes
+  const int N = T >> kFusedBits;   // GEMM columns
+  const int lgN = m - kFusedBits;
+  const uint32_t bk = uint32_t(N) * 16u;  // B: bytes between K-blocks of 8
+  uint8_t* sA = sm;
+  uint8_t* sBh = sA + P.nops * kFusedABytes;
+  uint8_t* sBl = sBh + N * 256;
+  float* buf0 = reinterpret_cast<float*>(sBl + N * 256);  // interleaved (re, im)
+  float* buf1 = buf0 + 2 * T;
+  uint16_t* dp = reinterpret_cast<uint16_t*>(buf1 + 2 * T);  // [nops][64]
+  uint16_t* dn = dp + kFusedMaxOps * 64;                      // [nops][256]
+  uint64_t* gk = reinterpret_cast<uint64_t*>(dn + kFusedMaxOps * 256);  // [8] chunk-row offsets
+  uint64_t* mbar = gk + 8;
+  uint32_t* tmem_base = reinterpret_cast<uint32_t*>(mbar + 1);
+
+  for (int o = 0; o < P.nops; ++o) {
+    const uint4* src = reinterpret_cast<const uint4*>(a_all + size_t(P.part[o]) * kFusedABytes);
+    uint4* dst = reinterpret_cast<uint4*>(sA + o * kFusedABytes);
+    for (int i = t; i < kFusedABytes / 16; i += kK4Threads) dst[i] = src[i];
+  }
+  for (int o = 0; o < P.nops; ++o) {
+    uint32_t pmask = 0;
+    for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[o][b];
+    for (int p = t; p < 64; p += kK4Threads) {
+      uint32_t x = 0;
+      for (int b = 0; b < kFusedBits; ++b) x |= uint32_t((p >> b) & 1) << P.pbits[o][b];
+      dp[o * 64 + p] = uint16_t(tswz(x));
+    }
+    for (int nn = t; nn < N; nn += kK4Threads) {
+      uint32_t x = 0, bit = 0;
+      for (int b = 0; b < m; ++b)
+        if (!((pmask >> b) & 1)) x |= uint32_t((nn >> bit++) & 1) << b;
+      dn[o * 256 + nn] = uint16_t(tswz(x));
+    }
+  }
+  // chunk c = t + r*256 holds tile indices 2c, 2c+1 (tile bit 0 is slot 0);
+  // its global index is dep(2t) + dep(2*r*256)
+  const int chunks = T / 2, rows = chunks / kK4Threads;
+  for (int r = t; r < rows; r += kK4Threads) gk[r] = dep(uint64_t(r) * kK4Threads * 2, P.tile);
+  if (t == 0) tc::mbar_init(mbar, 1);
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_base, 256);
+    tc::tmem_relinquish();
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_base;
+  const uint64_t gt = dep(uint64_t(t) * 2, P.tile);
+  const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
+  const uint32_t sb[2] = {tc::smem_u32(buf0), tc::smem_u32(buf1)};
+  uint32_t phase = 0;
+  bool failed = false;
+
+  auto issue_load = [&](uint64_t tl, uint32_t dst) {
+    const uint64_t gb = dep(tl, P.outer);
+    for (int r = 0; r < rows; ++r)
+      cp_async16(dst + tswz(2u * uint32_t(t + r * kK4Threads)) * 8u, sv + gb + gt + gk[r]);
+    (void)0;
+  };
+  uint64_t tile = blockIdx.x;
+  if (tile < P.ntiles) issue_load(tile, sb[0]);
+  cp_async_commit();
+  for (int it = 0; tile < P.ntiles; ++it, tile += gridDim.x) {
+    const uint64_t next = tile + gridDim.x;
+    if (next < P.ntiles) issue_load(next, sb[(it + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    float* X = (it & 1) ? buf1 : buf0;
+    const uint64_t gbase = dep(tile, P.outer);
+    for (int o = 0; o < P.nops; ++o) {
+      // B (N x 128, K-major), k = 2p + c: Re (c=0) / Im (c=1) of part index p.
+      // Item (kb, nn): K-block kb (part indices 4kb..4kb+3) of column nn; lanes
+      // run over consecutive columns, i.e. over the low tile bits.
+      for (int item = t; item < N * 16; item += kK4Threads) {
+        const int kb = item >> lgN, nn = item & (N - 1);
+        const uint32_t col = dn[o * 256 + nn];
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 x = *reinterpret_cast<const float2*>(X + 2 * (dp[o * 64 + 4 * kb + q] ^ col));
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(x.x - hf.x, x.y - hf.y);
+          hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+          lw[q] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+        const uint32_t off = tc::kmajor_off(uint32_t(nn), uint32_t(kb * 8), bk);
+        *reinterpret_cast<uint4*>(sBh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(sBl + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+      }
+      tc::fence_proxy_async_smem();
+      __syncthreads();
+      if (t == 0) {
+        tc::tc_fence_after();
+        const uint32_t a0 = tc::smem_u32(sA + o * kFusedABytes);
+        const uint32_t bh = tc::smem_u32(sBh), bl = tc::smem_u32(sBl);
+        const int nprod = P.precision == 1 ? 1 : 3;
+        uint32_t acc = 0;
+        for (int prod = 0; prod < nprod; ++prod) {
+          const uint32_t abase = a0 + (prod == 2 ? uint32_t(kFusedABytes / 2) : 0u);  // Al: third
+          const uint32_t bbase = prod == 1 ? bl : bh;                                 // Bl: second
+          for (int s = 0; s < 8; ++s) {  // K = 128 in steps of 16 (two 8-wide blocks)
+            const uint64_t ad = tc::smem_desc(abase + uint32_t(s) * 2u * 2048u, 2048u, 128u);
+            const uint64_t bd = tc::smem_desc(bbase + uint32_t(s) * 2u * bk, bk, 128u);
+            tc::mma_bf16(tmem, ad, bd, idesc, acc);
+            acc = 1;
+          }
+        }
+        tc::mma_commit(mbar);
+      }
+      const bool ok = tc::mbar_wait(mbar, phase, kWaitLimit);
+      if (__syncthreads_or(!ok)) {  // block-uniform decision
+        failed = true;
+        if (t == 0) atomicExch(err, 1);
+        tc::mbar_wait(mbar, phase, kWaitLimit);  // give the MMAs a last bounded chance
+        break;
+      }
+      phase ^= 1u;
+      tc::tc_fence_after();
+      {
+        // D row r = 2p + c (TMEM lane r): Re (c=0) / Im (c=1) of part index p.
+        // Warp w reads lanes 32*(w%4).. and half of the columns, 16 at a time
+        // (with N = 16 the second half-group idles).
+        const int quad = warp & 3, half = warp >> 2;
+        const int r = quad * 32 + lane;
+        const int comp = r & 1;
+        const uint32_t prow = dp[o * 64 + (r >> 1)];
+        const int per_half = N / 2 < 16 ? 16 : N / 2;
+        const int c_begin = half * per_half;
+        const int c_end = c_begin + per_half < N ? c_begin + per_half : N;
+        for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
+          float d[16];
+          tc::tmem_ld16(tmem + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
+          // the 16 column positions are the same for every lane: read them as
+          // eight broadcast 32-bit words
+          const uint32_t* cw = reinterpret_cast<const uint32_t*>(dn + o * 256 + c0);
+#pragma unroll
+          for (int j = 0; j < 16; j += 2) {
+            const uint32_t w = cw[j >> 1];
+            X[2 * (prow ^ (w & 0xffffu)) + comp] = d[j];
+            X[2 * (prow ^ (w >> 16)) + comp] = d[j + 1];
+          }
+        }
+      }
+      tc::tc_fence_before();
+      __syncthreads();
+    }
+    if (failed) break;
+    // write the tile back: 16-byte chunks, coalesced
+    for (int r = 0; r < rows; ++r) {
+      const uint4 d = *reinterpret_cast<const uint4*>(X + 2 * tswz(2u * uint32_t(t + r * kK4Threads)));
+      __stcs(reinterpret_cast<uint4*>(sv + gbase + gt + gk[r]), d);
+    }
+    __syncthreads();  // this buffer is refilled by the prefetch issued next iteration
+  }
+  cp_async_wait0();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+}
+
+}  // namespace
+
+int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, double2* d_u,
+                   void* d_a, cudaStream_t s) {
+  if (nparts <= 0) return HS_OK;
+  static bool attr = false;
+  if (!attr) {
+    HS_CUDA(cudaFuncSetAttribute(k5_compose, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(double2) * kFusedDim * kFusedDim)));
+    attr = true;
+  }
+  k5_compose<<<nparts, kFusedDim, sizeof(double2) * kFusedDim * kFusedDim, s>>>(
+      d_gates, d_offs, d_u, static_cast<uint8_t*>(d_a));
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
+int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    HS_CUDA(cudaFuncSetAttribute(k4_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr = true;
+  }
+  const int T = 1 << P.m, N = T >> kFusedBits;
+  const size_t smem = size_t(P.nops) * kFusedABytes + size_t(N) * 512 + size_t(T) * 16 +
+                      2 * (kFusedMaxOps * 64 + kFusedMaxOps * 256) + 8 * 8 + 8 + 8 + 16;
+  if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 pass needs %zu B of shared memory", smem);
+  int sms = 148;
+  int dev = 0;
+  HS_CUDA(cudaGetDevice(&dev));
+  HS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int grid = int(P.ntiles < uint64_t(sms) ? P.ntiles : uint64_t(sms));
+  k4_fused<<<grid, kK4Threads, smem, s>>>(static_cast<float2*>(amp), P,
+                                          static_cast<const uint8_t*>(d_a), d_err);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
+}  // namespace hisv

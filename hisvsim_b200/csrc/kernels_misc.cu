@@ -224,7 +224,81 @@ int grid_for(uint64_t size, int threads) {
   return int(std::max<uint64_t>(1, std::min(want, need)));
 }
 
+// <a|b>, max|a-b| and <b|b> over two states of possibly different precision
+template <typename VA, typename VB>
+__global__ void __launch_bounds__(kRedThreads) k3_compare(const VA* __restrict__ a,
+                                                          const VB* __restrict__ b, uint64_t size,
+                                                          double* __restrict__ partial) {
+  __shared__ double sh[kRedThreads / 32];
+  double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < size; i += stride) {
+    const double2 u = ld2(a, i), w = ld2(b, i);
+    s0 += u.x * w.x + u.y * w.y;
+    s1 += u.x * w.y - u.y * w.x;
+    const double dx = u.x - w.x, dy = u.y - w.y;
+    s2 = fmax(s2, sqrt(dx * dx + dy * dy));
+    s3 += w.x * w.x + w.y * w.y;
+  }
+  const double r0 = block_sum(s0, sh), r1 = block_sum(s1, sh), r3 = block_sum(s3, sh);
+  const double r2 = block_max(s2, sh);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = r0;
+    partial[gridDim.x + blockIdx.x] = r1;
+    partial[2 * gridDim.x + blockIdx.x] = r2;
+    partial[3 * gridDim.x + blockIdx.x] = r3;
+  }
+}
+
+__global__ void k3_compare_finish(const double* __restrict__ partial, int nblocks,
+                                  double* __restrict__ out) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int k = 0; k < 4; ++k) {
+    double s = 0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+      const double v = partial[k * nblocks + i];
+      s = k == 2 ? fmax(s, v) : s + v;
+    }
+    const double r = k == 2 ? block_max(s, sh) : block_sum(s, sh);
+    if (threadIdx.x == 0) out[k] = r;
+  }
+}
+
+template <typename VA, typename VB>
+int run_compare(const void* a, const void* b, uint64_t size, double out[4], cudaStream_t s) {
+  const int blocks = int(std::min<uint64_t>(kRedBlocks, (size + kRedThreads - 1) / kRedThreads));
+  double* scratch = nullptr;
+  HS_CUDA(cudaMallocAsync(&scratch, sizeof(double) * (4 * blocks + 4), s));
+  k3_compare<VA, VB><<<blocks, kRedThreads, 0, s>>>(static_cast<const VA*>(a),
+                                                    static_cast<const VB*>(b), size, scratch);
+  k3_compare_finish<<<1, kRedThreads, 0, s>>>(scratch, blocks, scratch + 4 * blocks);
+  cudaError_t e1 = cudaGetLastError();
+  cudaError_t e2 = cudaMemcpyAsync(out, scratch + 4 * blocks, 4 * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s);
+  cudaError_t e3 = cudaFreeAsync(scratch, s);
+  cudaError_t e4 = cudaStreamSynchronize(s);
+  for (cudaError_t e : {e1, e2, e3, e4})
+    if (e != cudaSuccess) return set_error(HS_E_CUDA, "compare: %s", cudaGetErrorString(e));
+  return HS_OK;
+}
+
 }  // namespace
+
+int reduce_compare(const void* a, int adtype, const void* b, int bdtype, int n, double out[4],
+                   cudaStream_t s) {
+  return reduce_compare_count(a, adtype, b, bdtype, 1ull << n, out, s);
+}
+
+int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, uint64_t count,
+                         double out[4], cudaStream_t s) {
+  if (adtype == HS_DTYPE_C128 && bdtype == HS_DTYPE_C128)
+    return run_compare<double2, double2>(a, b, count, out, s);
+  if (adtype == HS_DTYPE_C128 && bdtype == HS_DTYPE_C64)
+    return run_compare<double2, float2>(a, b, count, out, s);
+  if (adtype == HS_DTYPE_C64 && bdtype == HS_DTYPE_C128)
+    return run_compare<float2, double2>(a, b, count, out, s);
+  return run_compare<float2, float2>(a, b, count, out, s);
+}
 
 int reduce_chunks(const void* amp, int dtype, int n, int chunk_bits, double* host_out,
                   cudaStream_t s) {

@@ -175,6 +175,32 @@ int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates
 /* Tile-size override for K1 (0 = automatic).  Returns the previous value. */
 int hs_set_tile_qubits(int m);
 
+/* ---- precision form (complex64 state, fused unitaries on the tensor cores) --
+ * No counterpart in the reference: each part (<= 6 qubits) becomes one 64x64
+ * unitary composed in FP64 (K5), applied to a complex64 state by K4 as a real
+ * 128x128 GEMM on the tcgen05 tensor cores with split-BF16 operands and FP32
+ * accumulation, up to two unitaries per state pass.  Parts have the meaning of
+ * gather_and_execute_on's gate lists (execute.hpp:171). */
+#define HS_FUSED_BF16X3 0 /* Ah*Bh + Ah*Bl + Al*Bh: ~2^-16 relative per product */
+#define HS_FUSED_BF16X1 1 /* one BF16 product (fast, ~2^-8) */
+int hs_fused_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
+                       int num_parts, int precision, void* stream);
+/* K5 alone, for checking: the FP64 unitaries of the parts on an n-qubit
+ * register with identity slot map.  out_u: num_parts x 64 x 64 complex128
+ * (row-major, row = output basis index); out_qubits: num_parts x 6, the qubit
+ * of each local bit (bit j = j-th lowest slot; parts smaller than six qubits
+ * are padded with the lowest other qubits). */
+int hs_fused_compose(int num_qubits, const hs_gate* gates, const int32_t* part_offsets,
+                     int num_parts, double* out_u, int32_t* out_qubits);
+/* out = {Re<a|b>, Im<a|b>, max|a-b|, <b|b>} in FP64 for states of any two
+ * precisions (slot maps are brought to the identity first): the fidelity
+ * |<a|b>|^2 / (<a|a><b|b>) and max amplitude error of the precision form. */
+int hs_compare(hs_state* a, hs_state* b, double out[4]);
+/* Same as hs_compare with b given as 2^n host amplitudes in qubit order (of
+ * dtype bdtype), streamed through the device in 2^26-amplitude chunks: for
+ * comparisons whose two states do not fit in HBM together. */
+int hs_compare_host(hs_state* a, const void* host_b, int bdtype, double out[4]);
+
 /* ---- redistribution (svsim-mpi.hpp:123-173, mpi_redistributer.hpp:100-344) */
 
 /* In-place bit-swap pass (K2): exchange slot bits pairs[2i] <-> pairs[2i+1]

@@ -1,0 +1,105 @@
+"""Precision form: FP64-composed 64x64 unitaries (K5) applied to complex64
+states on the tensor cores with split-BF16 operands (K4).
+
+Tolerances: composed unitaries match the oracle to 1e-12; the complex64
+result keeps fidelity loss 1 - |<psi_fp64|psi>|^2 <= 1e-6
+and max amplitude error <= 1e-5 against complex128."""
+import numpy as np
+import pytest
+
+from hisvsim_b200 import abi, circuits, partition
+from hisvsim_b200.gates import Gate, part_offsets, to_records
+
+pytestmark = pytest.mark.gpu
+
+
+def fid(a, b):
+    return abs(np.vdot(a, b)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real)
+
+
+def test_compose_matches_oracle(port):
+    n = 8
+    gates = circuits.random_layered(n, 4, 3) + [Gate("RXX", (1, 4), params=(0.4,)),
+                                                Gate("SWAP", (2, 5), (0,))]
+    parts = partition.partition_acyclic(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    U, Q = abi.fused_compose(n, rec, offs)
+    for p in range(len(parts)):
+        pg = to_records([gates[i] for i in parts[p]])
+        place = lambda j: sum(((j >> b) & 1) << int(Q[p][b]) for b in range(6))
+        for j in range(64):
+            init = np.zeros(1 << n, complex)
+            init[place(j)] = 1
+            out = port.run(n, pg, init_state=init)
+            col = np.array([out[place(i)] for i in range(64)])
+            assert np.abs(col - U[p][:, j]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("n", [10, 11, 12, 14, 16])
+def test_fused_against_oracle(port, n):
+    gates = circuits.random_u3_cz(n, 6, 5)
+    parts = partition.partition_acyclic(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    st = abi.State(n, abi.C64)
+    st.run_fused(rec, offs, 0)  # three BF16 products
+    got = st.amplitudes().astype(complex)
+    assert 1 - fid(want, got) <= 1e-8
+    assert np.abs(got - want).max() <= 1e-5
+
+
+def test_fused_all_gate_kinds(port):
+    n = 12
+    import tests.golden.make_golden as mg
+
+    gates = [g for g in mg.all_gate_circuit(n, 120, 77) if len(set(g.qubits)) <= 6]
+    parts = partition.partition_acyclic(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    st = abi.State(n, abi.C64)
+    st.run_fused(rec, offs)
+    got = st.amplitudes().astype(complex)
+    # the all-gate mix is not unitary (C1 / C2 with arbitrary entries): compare
+    # directions and relative error
+    assert 1 - fid(want, got) <= 1e-8
+    assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
+
+
+def test_single_product_is_coarser(port):
+    n = 12
+    gates = circuits.random_u3_cz(n, 6, 6)
+    parts = partition.partition_acyclic(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    st = abi.State(n, abi.C64)
+    st.run_fused(rec, offs, 1)
+    loss = 1 - fid(want, st.amplitudes().astype(complex))
+    assert 1e-9 < loss <= 1e-3
+
+
+def test_fused_28q_against_plain_complex128():
+    n = 28
+    gates = circuits.random_u3_cz(n, 10, 1)
+    fparts = partition.partition_acyclic(gates, 6)
+    frec, foffs = part_offsets(partition.parts_to_gates(gates, fparts))
+    pparts = partition.partition_acyclic(gates, 9)
+    prec, poffs = part_offsets(partition.parts_to_gates(gates, pparts))
+    f = abi.State(n, abi.C64)
+    f.run_fused(frec, foffs)
+    p = abi.State(n, abi.C128)
+    p.run_parts(prec, poffs)
+    c = p.compare(f)
+    assert 1 - c["fidelity"] <= 1e-6
+    assert c["max_abs_diff"] <= 1e-5
+    h = p.compare_host(f.raw())
+    assert abs(h["fidelity"] - c["fidelity"]) <= 1e-12
+
+
+def test_fused_errors():
+    with pytest.raises(abi.HisvError):
+        abi.State(12, abi.C128).run_fused(to_records([Gate("H", (0,))]), np.array([0, 1]))
+    with pytest.raises(abi.HisvError):
+        abi.State(8, abi.C64).run_fused(to_records([Gate("H", (0,))]), np.array([0, 1]))
+    big = [Gate("X", (q,)) for q in range(7)]
+    with pytest.raises(abi.HisvError):
+        abi.State(12, abi.C64).run_fused(to_records(big), np.array([0, 7]))
