@@ -68,6 +68,27 @@ SIGNATURES = {
     "hs_fused_compose": [_i, _vp, _vp, _i, _vp, _vp],
     "hs_compare": [_vp, _vp, _dp],
     "hs_compare_host": [_vp, _vp, _i, _dp],
+    "hs_batch_create_qaoa": [_i, _vp, _vp, _vp, _i, _vp, _vp, ctypes.POINTER(_vp)],
+    "hs_batch_set_params": [_vp, _vp, _vp],
+    "hs_batch_configure": [_vp, _i, _i],
+    "hs_batch_tune": [_vp, _vp, _vp, _dp],
+    "hs_batch_run": [_vp, _vp, _dp],
+    "hs_batch_stats": [_vp, _vp],
+    "hs_batch_tile_caps": [_vp, _vp],
+    "hs_batch_state": [_vp, _i, _vp],
+    "hs_batch_destroy": [_vp],
+    "hs_mlp_create": [_i, ctypes.c_uint64, ctypes.POINTER(_vp)],
+    "hs_mlp_num_params": [_vp],
+    "hs_mlp_get_params": [_vp, _vp],
+    "hs_mlp_set_params": [_vp, _vp],
+    "hs_mlp_predict": [_vp, _vp, _i, _vp],
+    "hs_mlp_gradients": [_vp, _vp, _vp, _i, _vp, _vp],
+    "hs_mlp_train": [_vp, _vp, _vp, _i, _i, _i, ctypes.c_float, ctypes.c_uint64, _vp],
+    "hs_mlp_destroy": [_vp],
+    "hs_num_part_features": [],
+    "hs_part_features": [_i, _i, _vp, _i, _vp, _vp, _i, _vp],
+    "hs_order_segments": [_i, _i, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _vp],
+    "hs_parts_run_timed": [_vp, _vp, _vp, _i, _vp, _vp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
@@ -195,6 +216,15 @@ class State:
         offsets = np.ascontiguousarray(offsets, dtype=np.int32)
         check(lib().hs_parts_run(self.h, _ptr(records), _ptr(offsets), len(offsets) - 1, stream))
 
+    def run_parts_timed(self, records: np.ndarray, offsets: np.ndarray, stream=None) -> np.ndarray:
+        """run_parts with per-part device times (ms)."""
+        records = _records(records)
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        ms = np.zeros(len(offsets) - 1, dtype=np.float32)
+        check(lib().hs_parts_run_timed(self.h, _ptr(records), _ptr(offsets), len(offsets) - 1,
+                                       _ptr(ms), stream))
+        return ms
+
     def run_fused(self, records: np.ndarray, offsets: np.ndarray, precision: int = 0,
                   stream=None):
         """Precision form: one fused unitary per part, tensor-core GEMMs (complex64)."""
@@ -273,6 +303,39 @@ def plan_stats(n: int, gates, dtype: int = C128) -> dict:
     return dict(zip(["passes", "groups", "ops", "dense", "diag", "tile_bits"], out.tolist()))
 
 
+def num_part_features() -> int:
+    return lib().hs_num_part_features()
+
+
+def part_features(n: int, gates, parts, dtype: int = C64) -> np.ndarray:
+    """Cost-model features (host only) of parts given as gate index lists."""
+    rec = _records(gates)
+    offs = np.zeros(len(parts) + 1, dtype=np.int32)
+    np.cumsum([len(p) for p in parts], out=offs[1:])
+    idx = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int32) for p in parts])
+                               if parts else np.zeros(0, dtype=np.int32), dtype=np.int32)
+    out = np.zeros((len(parts), num_part_features()), dtype=np.float32)
+    check(lib().hs_part_features(n, dtype, _ptr(rec), len(rec), _ptr(idx), _ptr(offs), len(parts),
+                                 _ptr(out)))
+    return out
+
+
+def order_segments(n: int, gates, order, max_qubits: int, max_len: int, dtype: int = C64):
+    """All contiguous segments of a topological order under the limits:
+    (start, length, features)."""
+    rec = _records(gates)
+    order = np.ascontiguousarray(order, dtype=np.int32)
+    cap = len(order) * max_len
+    st = np.zeros(cap, dtype=np.int32)
+    ln = np.zeros(cap, dtype=np.int32)
+    ft = np.zeros((cap, num_part_features()), dtype=np.float32)
+    cnt = ctypes.c_int32()
+    check(lib().hs_order_segments(n, dtype, _ptr(rec), len(rec), _ptr(order), max_qubits, max_len,
+                                  cap, _ptr(st), _ptr(ln), _ptr(ft), ctypes.byref(cnt)))
+    c = cnt.value
+    return st[:c], ln[:c], ft[:c]
+
+
 def fused_compose(n: int, records: np.ndarray, offsets: np.ndarray):
     """K5 only: FP64 unitaries (parts x 64 x 64) and the qubit of each local bit."""
     records = _records(records)
@@ -323,6 +386,129 @@ def launch_bytes() -> int:
 
 def set_timing(on: bool) -> int:
     return lib().hs_set_timing(1 if on else 0)
+
+
+class Mlp:
+    """Learned cost model: in_dim -> 64 -> 64 -> 64 -> 1 (ReLU, FP32) on the GPU."""
+
+    def __init__(self, in_dim: int, seed: int = 0):
+        h = _vp()
+        check(lib().hs_mlp_create(in_dim, seed, ctypes.byref(h)))
+        self.h = h
+        self.in_dim = in_dim
+        self.num_params = lib().hs_mlp_num_params(h)
+
+    @staticmethod
+    def _f32(a, shape=None):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        return a if shape is None else a.reshape(shape)
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.num_params, dtype=np.float32)
+        check(lib().hs_mlp_get_params(self.h, _ptr(out)))
+        return out
+
+    def set_params(self, p):
+        p = self._f32(p, (self.num_params,))
+        check(lib().hs_mlp_set_params(self.h, _ptr(p)))
+
+    def predict(self, x) -> np.ndarray:
+        x = self._f32(x, (-1, self.in_dim))
+        out = np.empty(len(x), dtype=np.float32)
+        check(lib().hs_mlp_predict(self.h, _ptr(x), len(x), _ptr(out)))
+        return out
+
+    def gradients(self, x, y):
+        x = self._f32(x, (-1, self.in_dim))
+        y = self._f32(y, (-1,))
+        g = np.empty(self.num_params, dtype=np.float32)
+        loss = ctypes.c_float()
+        check(lib().hs_mlp_gradients(self.h, _ptr(x), _ptr(y), len(x), _ptr(g),
+                                     ctypes.byref(loss)))
+        return loss.value, g
+
+    def train(self, x, y, epochs: int, batch: int = 256, lr: float = 1e-3, seed: int = 0):
+        x = self._f32(x, (-1, self.in_dim))
+        y = self._f32(y, (-1,))
+        losses = np.zeros(max(epochs, 1), dtype=np.float32)
+        check(lib().hs_mlp_train(self.h, _ptr(x), _ptr(y), len(x), epochs, batch, lr, seed,
+                                 _ptr(losses)))
+        return losses[:epochs]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hs_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class QaoaBatch:
+    """Batching form: many QAOA MaxCut instances in one persistent launch."""
+
+    def __init__(self, instances, p: int):
+        """instances: list of (n, edges, gammas[p], betas[p])."""
+        self.n = np.array([int(i[0]) for i in instances], dtype=np.int32)
+        offs = np.zeros(len(instances) + 1, dtype=np.int32)
+        np.cumsum([len(i[1]) for i in instances], out=offs[1:])
+        edges = np.array([e for i in instances for e in i[1]], dtype=np.int32).reshape(-1)
+        g = np.array([i[2] for i in instances], dtype=np.float64).reshape(-1)
+        b = np.array([i[3] for i in instances], dtype=np.float64).reshape(-1)
+        h = _vp()
+        check(lib().hs_batch_create_qaoa(len(instances), _ptr(self.n), _ptr(offs), _ptr(edges), p,
+                                         _ptr(g), _ptr(b), ctypes.byref(h)))
+        self.h = h
+        self.p = p
+        self.count = len(instances)
+
+    def set_params(self, gammas, betas):
+        g = np.ascontiguousarray(gammas, dtype=np.float64).reshape(-1)
+        b = np.ascontiguousarray(betas, dtype=np.float64).reshape(-1)
+        check(lib().hs_batch_set_params(self.h, _ptr(g), _ptr(b)))
+
+    def configure(self, tile_cap: int, ctas_per_sm: int):
+        check(lib().hs_batch_configure(self.h, tile_cap, ctas_per_sm))
+
+    def tune(self):
+        cap, ctas, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        check(lib().hs_batch_tune(self.h, ctypes.byref(cap), ctypes.byref(ctas), ctypes.byref(ms)))
+        return cap.value, ctas.value, ms.value
+
+    def run(self):
+        out = np.zeros(self.count)
+        ms = ctypes.c_double()
+        check(lib().hs_batch_run(self.h, out.ctypes.data_as(_dp), ctypes.byref(ms)))
+        return out, ms.value
+
+    def stats(self):
+        s = np.zeros(5, dtype=np.int64)
+        check(lib().hs_batch_stats(self.h, _ptr(s)))
+        return dict(zip(["items", "steps", "bytes_per_run", "tile_cap", "ctas_per_sm"], s.tolist()))
+
+    def tile_caps(self) -> np.ndarray:
+        caps = np.zeros(self.count, dtype=np.int32)
+        check(lib().hs_batch_tile_caps(self.h, _ptr(caps)))
+        return caps
+
+    def state(self, i: int) -> np.ndarray:
+        out = np.empty(1 << int(self.n[i]), dtype=np.complex64)
+        check(lib().hs_batch_state(self.h, i, _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hs_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def set_tile_qubits(m: int) -> int:

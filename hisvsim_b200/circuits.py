@@ -108,14 +108,39 @@ def random_regular3(n: int, rng: np.random.Generator, tries: int = 1000) -> List
     raise RuntimeError("could not draw a simple 3-regular graph")
 
 
+def random_maxcut_graph(n: int, rng: np.random.Generator, tries: int = 1000) -> List[Tuple[int, int]]:
+    """Random simple 3-regular graph for even n; for odd n (no 3-regular graph
+    exists) the same pairing model with one vertex of degree 2, so every qubit
+    stays coupled and |E| = (3n - 1) / 2."""
+    if n % 2 == 0:
+        return random_regular3(n, rng, tries)
+    if n < 5:
+        raise ValueError("need n >= 5 for an odd near-3-regular graph")
+    for _ in range(tries):
+        deg = np.full(n, 3)
+        deg[int(rng.integers(n))] = 2
+        stubs = rng.permutation(np.repeat(np.arange(n), deg))
+        edges = set()
+        ok = True
+        for k in range(0, len(stubs), 2):
+            a, b = int(stubs[k]), int(stubs[k + 1])
+            if a == b or (min(a, b), max(a, b)) in edges:
+                ok = False
+                break
+            edges.add((min(a, b), max(a, b)))
+        if ok:
+            return sorted(edges)
+    raise RuntimeError("could not draw a simple near-3-regular graph")
+
+
 def qaoa_maxcut(n: int, p: int, seed: int):
-    """QAOA MaxCut on a random 3-regular graph.
+    """QAOA MaxCut on a random 3-regular graph (near-3-regular for odd n).
 
     Returns (gates, edges, gammas, betas); gates start with H on every qubit
     (|+>^n), then per round RZZ(gamma) on each edge and RX(2 beta) on each qubit.
     """
     rng = np.random.default_rng(seed)
-    edges = random_regular3(n, rng)
+    edges = random_maxcut_graph(n, rng)
     gammas = rng.uniform(0, math.pi, p)
     betas = rng.uniform(0, math.pi / 2, p)
     out: List[Gate] = [Gate("H", (q,)) for q in range(n)]

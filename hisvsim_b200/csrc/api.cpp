@@ -25,6 +25,7 @@ int set_error(int code, const char* fmt, ...) {
 
 static std::atomic<long long> g_gates{0}, g_passes{0}, g_param_bytes{0};
 static std::atomic<int> g_tile_hint{0};
+int current_tile_hint() { return g_tile_hint.load(); }
 
 // device-time accounting of K1/K2 launches: event pairs resolved when read
 static std::mutex g_ev_mu;
@@ -332,6 +333,47 @@ int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets
   for (int p = 0; p < num_parts; ++p)
     HS_TRY(run_lowered(st, all[p], part_offsets[p + 1] - part_offsets[p], S(stream)));
   return HS_OK;
+}
+
+int hs_parts_run_timed(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
+                       int num_parts, float* part_ms, void* stream) {
+  HS_TRY(check_state(st));
+  if (num_parts < 0 || (num_parts > 0 && (!gates || !part_offsets || !part_ms)))
+    return set_error(HS_E_INVALID, "bad part list");
+  for (int p = 0; p < num_parts; ++p)
+    if (part_offsets[p + 1] < part_offsets[p] || part_offsets[p] < 0)
+      return set_error(HS_E_INVALID, "part offsets must be non-decreasing");
+  // plan every part before the first launch, so that the device never waits
+  // for the host between two parts and each event pair brackets one part only
+  std::vector<std::vector<PartProgram>> progs(num_parts);
+  for (int p = 0; p < num_parts; ++p) {
+    std::vector<LoweredGate> lg;
+    HS_TRY(lower_all(st, gates + part_offsets[p], part_offsets[p + 1] - part_offsets[p], &lg));
+    HS_TRY(plan_part(st->n, st->q2s, lg, g_tile_hint.load(), st->dtype, &progs[p]));
+  }
+  std::vector<cudaEvent_t> ev(num_parts + 1, nullptr);
+  int rc = HS_OK;
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) rc = set_error(HS_E_CUDA, "event create");
+  const cudaStream_t s = S(stream);
+  if (rc == HS_OK && cudaEventRecord(ev[0], s) != cudaSuccess)
+    rc = set_error(HS_E_CUDA, "event record");
+  for (int p = 0; p < num_parts && rc == HS_OK; ++p) {
+    for (const auto& pr : progs[p]) {
+      if ((rc = launch_part(st->amp, st->dtype, pr, s)) != HS_OK) break;
+      count_pass(pr.nops);
+    }
+    if (rc == HS_OK && cudaEventRecord(ev[p + 1], s) != cudaSuccess)
+      rc = set_error(HS_E_CUDA, "event record");
+  }
+  if (rc == HS_OK && cudaStreamSynchronize(s) != cudaSuccess)
+    rc = set_error(HS_E_CUDA, "synchronize");
+  for (int p = 0; p < num_parts && rc == HS_OK; ++p)
+    if (cudaEventElapsedTime(&part_ms[p], ev[p], ev[p + 1]) != cudaSuccess)
+      rc = set_error(HS_E_CUDA, "elapsed time");
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  return rc;
 }
 
 int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates,

@@ -1,0 +1,435 @@
+// Host side of the batching form (hs_batch_*): instance layout, pass planning,
+// the work queue, CUDA-graph capture of one whole batch run, and the
+// autotuner that picks the tile size and the CTA count by timing.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+using namespace hisv;
+
+struct hs_batch {
+  int ninst = 0, p = 0, max_n = 0;
+  std::vector<int> n;
+  std::vector<std::vector<std::pair<int, int>>> edges;
+  std::vector<double> gammas, betas;
+  int tile_cap = 12, ctas_per_sm = 4;
+  int cap_of_n[kBatchMaxQubits + 1] = {};  // per qubit count; 0 = tile_cap
+  void* pool = nullptr;
+  std::vector<uint64_t> offset;  // amplitude offset of each instance in the pool
+  BatchInstance* d_inst = nullptr;
+  BatchParams* d_par = nullptr;
+  BatchItem* d_items = nullptr;
+  uint32_t* d_counters = nullptr;
+  unsigned long long* d_head = nullptr;
+  int* d_err = nullptr;
+  double* d_partial = nullptr;
+  double* d_expect = nullptr;
+  double* h_expect = nullptr;
+  int* h_err = nullptr;
+  int ngroups = 0;
+  uint64_t total = 0, ncounters = 0, pass_bytes = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void free_plan(hs_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  for (void* p : {(void*)b->d_inst, (void*)b->d_items, (void*)b->d_counters, (void*)b->d_partial})
+    if (p) cudaFree(p);
+  b->d_inst = nullptr;
+  b->d_items = nullptr;
+  b->d_counters = nullptr;
+  b->d_partial = nullptr;
+}
+
+void runs(const std::vector<int>& dst, Runs* r) {
+  r->n = 0;
+  size_t i = 0;
+  while (i < dst.size()) {
+    size_t j = i + 1;
+    while (j < dst.size() && dst[j] == dst[j - 1] + 1) ++j;
+    r->src[r->n] = uint8_t(i);
+    r->len[r->n] = uint8_t(j - i);
+    r->dst[r->n] = uint8_t(dst[i]);
+    ++r->n;
+    i = j;
+  }
+}
+
+// Passes of one round for n qubits with tiles of at most `cap` bits: pass 0
+// takes qubits [0, cap) and the cost phase; later passes keep slots 0..2 for
+// contiguity and mix the next cap-3 qubits.
+int plan_passes(int n, int cap, BatchInstance* I) {
+  std::vector<std::vector<int>> tiles, targets;
+  if (n <= cap) {
+    std::vector<int> all;
+    for (int q = 0; q < n; ++q) all.push_back(q);
+    tiles.push_back(all);
+    targets.push_back(all);
+  } else {
+    std::vector<int> t0;
+    for (int q = 0; q < cap; ++q) t0.push_back(q);
+    tiles.push_back(t0);
+    targets.push_back(t0);
+    int covered = cap;
+    while (covered < n) {
+      const int nw = std::min(cap - 3, n - covered);
+      std::vector<int> tl = {0, 1, 2}, tg;
+      for (int q = covered; q < covered + nw; ++q) {
+        tl.push_back(q);
+        tg.push_back(q);
+      }
+      tiles.push_back(tl);
+      targets.push_back(tg);
+      covered += nw;
+    }
+  }
+  if (int(tiles.size()) > kBatchMaxPasses)
+    return set_error(HS_E_UNSUPPORTED, "%d qubits need %d passes with %d-qubit tiles (max %d)", n,
+                     int(tiles.size()), cap, kBatchMaxPasses);
+  I->npasses = int(tiles.size());
+  for (int j = 0; j < I->npasses; ++j) {
+    BatchPass& P = I->pass[j];
+    std::memset(&P, 0, sizeof(P));
+    const std::vector<int>& tl = tiles[j];
+    P.m = int(tl.size());
+    runs(tl, &P.tile);
+    for (int b = 0; b < P.m; ++b) P.tile_slot[b] = uint8_t(tl[b]);
+    std::vector<int> outer;
+    for (int q = 0; q < n; ++q)
+      if (std::find(tl.begin(), tl.end(), q) == tl.end()) outer.push_back(q);
+    runs(outer, &P.outer);
+    P.phase = j == 0;
+    std::vector<int> tb;  // target tile bits
+    for (int q : targets[j]) tb.push_back(int(std::find(tl.begin(), tl.end(), q) - tl.begin()));
+    P.ngroups = int((tb.size() + 3) / 4);
+    for (int g = 0; g < P.ngroups; ++g) {
+      std::vector<int> regs;
+      for (size_t x = 4 * g; x < tb.size() && regs.size() < 4; ++x) regs.push_back(tb[x]);
+      const int ntg = int(regs.size());
+      for (int b = P.m - 1; b >= 0 && regs.size() < 4; --b)
+        if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
+      for (int k = 0; k < 4; ++k) P.group_bits[g][k] = uint8_t(regs[k]);
+      P.group_rx[g] = uint8_t((1 << ntg) - 1);
+    }
+  }
+  return HS_OK;
+}
+
+int upload_params(hs_batch* b) {
+  std::vector<BatchParams> par(b->ninst);
+  std::memset(par.data(), 0, sizeof(BatchParams) * par.size());
+  for (int i = 0; i < b->ninst; ++i) {
+    const int ne = int(b->edges[i].size());
+    for (int r = 0; r < b->p; ++r) {
+      const double beta = b->betas[size_t(i) * b->p + r], gamma = b->gammas[size_t(i) * b->p + r];
+      // RX(2 beta): cos(beta), -i sin(beta); RZZ(gamma) on every edge
+      par[i].rx[r][0] = make_float2(float(std::cos(beta)), float(std::sin(beta)));
+      for (int c = 0; c <= ne; ++c) {
+        const double ang = 0.5 * gamma * (2.0 * c - ne);
+        par[i].phase[r][c] = make_float2(float(std::cos(ang)), float(std::sin(ang)));
+      }
+    }
+  }
+  HS_CUDA(cudaMemcpy(b->d_par, par.data(), sizeof(BatchParams) * par.size(),
+                     cudaMemcpyHostToDevice));
+  return HS_OK;
+}
+
+int build_plan(hs_batch* b) {
+  free_plan(b);
+  std::vector<BatchInstance> inst(b->ninst);
+  std::memset(inst.data(), 0, sizeof(BatchInstance) * inst.size());
+  uint64_t nc = 0;
+  int maxsteps = 0;
+  b->pass_bytes = 0;
+  for (int i = 0; i < b->ninst; ++i) {
+    BatchInstance& I = inst[i];
+    I.amp = static_cast<float2*>(b->pool) + b->offset[i];
+    I.n = b->n[i];
+    I.p = b->p;
+    I.nedges = int(b->edges[i].size());
+    for (int e = 0; e < I.nedges; ++e) {
+      I.edge_a[e] = uint8_t(b->edges[i][e].first);
+      I.edge_b[e] = uint8_t(b->edges[i][e].second);
+    }
+    HS_TRY(plan_passes(I.n, b->cap_of_n[I.n] ? b->cap_of_n[I.n] : b->tile_cap, &I));
+    I.step_base = nc;
+    const int steps = I.npasses * b->p;
+    nc += uint64_t(steps);
+    maxsteps = std::max(maxsteps, steps);
+    b->pass_bytes += uint64_t(steps) * 2ull * (8ull << I.n);
+  }
+  std::vector<BatchItem> items;
+  uint64_t total = 0;
+  for (int k = 0; k < maxsteps; ++k)
+    for (int i = 0; i < b->ninst; ++i) {
+      const BatchInstance& I = inst[i];
+      if (k >= I.npasses * b->p) continue;
+      BatchItem it;
+      it.first = total;
+      it.inst = i;
+      it.step = k;
+      it.ntiles = uint32_t(1ull << (I.n - I.pass[k % I.npasses].m));
+      items.push_back(it);
+      total += it.ntiles;
+    }
+  b->ngroups = int(items.size());
+  b->total = total;
+  b->ncounters = nc;
+  const int max_chunks = 1 << (b->max_n > 16 ? b->max_n - 16 : 0);
+  HS_CUDA(cudaMalloc(&b->d_inst, sizeof(BatchInstance) * inst.size()));
+  HS_CUDA(cudaMalloc(&b->d_items, sizeof(BatchItem) * items.size()));
+  HS_CUDA(cudaMalloc(&b->d_counters, sizeof(uint32_t) * nc));
+  HS_CUDA(cudaMalloc(&b->d_partial, sizeof(double) * size_t(b->ninst) * max_chunks));
+  HS_CUDA(cudaMemcpy(b->d_inst, inst.data(), sizeof(BatchInstance) * inst.size(),
+                     cudaMemcpyHostToDevice));
+  HS_CUDA(cudaMemcpy(b->d_items, items.data(), sizeof(BatchItem) * items.size(),
+                     cudaMemcpyHostToDevice));
+  // one whole run as a CUDA graph: reset the queue, |+>^n, the persistent
+  // launch, <H_C>, and the read-back of results and error flag
+  int dev = 0, sms = 148;
+  HS_CUDA(cudaGetDevice(&dev));
+  HS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  HS_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(b->d_head, 0, sizeof(unsigned long long), b->stream);
+  cudaMemsetAsync(b->d_counters, 0, sizeof(uint32_t) * nc, b->stream);
+  cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream);
+  int rc = launch_batch_init(b->d_inst, b->ninst, b->stream);
+  if (rc == HS_OK)
+    rc = launch_batch(b->d_inst, b->d_par, b->d_items, b->ngroups, b->total, b->d_counters,
+                      b->d_head, b->d_err, sms * b->ctas_per_sm, b->stream);
+  if (rc == HS_OK)
+    rc = launch_batch_expect(b->d_inst, b->ninst, b->max_n, b->d_partial, b->d_expect, b->stream);
+  cudaMemcpyAsync(b->h_expect, b->d_expect, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost,
+                  b->stream);
+  cudaMemcpyAsync(b->h_err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc != HS_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_error(HS_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  b->graph = g;
+  HS_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+  return HS_OK;
+}
+
+int run_once(hs_batch* b, double* ms) {
+  if (!b->exec) return set_error(HS_E_INVALID, "batch has no plan");
+  HS_CUDA(cudaEventRecord(b->ev0, b->stream));
+  HS_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  HS_CUDA(cudaEventRecord(b->ev1, b->stream));
+  HS_CUDA(cudaStreamSynchronize(b->stream));
+  if (ms) {
+    float f = 0;
+    HS_CUDA(cudaEventElapsedTime(&f, b->ev0, b->ev1));
+    *ms = f;
+  }
+  if (*b->h_err) return set_error(HS_E_TIMEOUT, "a batch dependency wait timed out");
+  return HS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hs_batch_create_qaoa(int num_instances, const int32_t* num_qubits, const int32_t* edge_offsets,
+                         const int32_t* edges, int p, const double* gammas, const double* betas,
+                         hs_batch** out) {
+  if (!out) return set_error(HS_E_INVALID, "null output");
+  *out = nullptr;
+  if (num_instances < 1 || p < 1 || p > kBatchMaxRounds)
+    return set_error(HS_E_INVALID, "need >= 1 instance and 1..%d rounds", kBatchMaxRounds);
+  auto* b = new hs_batch;
+  b->ninst = num_instances;
+  b->p = p;
+  b->n.assign(num_qubits, num_qubits + num_instances);
+  b->edges.resize(num_instances);
+  uint64_t amps = 0;
+  for (int i = 0; i < num_instances; ++i) {
+    const int n = b->n[i];
+    if (n < 4 || n > kBatchMaxQubits) {
+      delete b;
+      return set_error(HS_E_INVALID, "instance %d: %d qubits outside 4..%d", i, n, kBatchMaxQubits);
+    }
+    const int ne = edge_offsets[i + 1] - edge_offsets[i];
+    if (ne < 0 || ne > kBatchMaxEdges) {
+      delete b;
+      return set_error(HS_E_INVALID, "instance %d: %d edges (max %d)", i, ne, kBatchMaxEdges);
+    }
+    for (int e = edge_offsets[i]; e < edge_offsets[i + 1]; ++e) {
+      const int a = edges[2 * e], c = edges[2 * e + 1];
+      if (a < 0 || c < 0 || a >= n || c >= n || a == c) {
+        delete b;
+        return set_error(HS_E_INVALID, "instance %d: bad edge (%d, %d)", i, a, c);
+      }
+      b->edges[i].push_back({a, c});
+    }
+    b->offset.push_back(amps);
+    amps += 1ull << n;
+    b->max_n = std::max(b->max_n, n);
+  }
+  b->gammas.assign(gammas, gammas + size_t(num_instances) * p);
+  b->betas.assign(betas, betas + size_t(num_instances) * p);
+  int rc = HS_OK;
+  auto fail = [&](int code) {
+    hs_batch_destroy(b);
+    return code;
+  };
+  if (cudaMalloc(&b->pool, amps * sizeof(float2)) != cudaSuccess) {
+    cudaGetLastError();
+    delete b;
+    return set_error(HS_E_NOMEM, "batch states: %llu amplitudes", (unsigned long long)amps);
+  }
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+      cudaMalloc(&b->d_par, sizeof(BatchParams) * num_instances) != cudaSuccess ||
+      cudaMalloc(&b->d_head, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_expect, sizeof(double) * num_instances) != cudaSuccess ||
+      cudaMallocHost(&b->h_expect, sizeof(double) * num_instances) != cudaSuccess ||
+      cudaMallocHost(&b->h_err, sizeof(int)) != cudaSuccess)
+    return fail(set_error(HS_E_NOMEM, "batch buffers"));
+  if ((rc = upload_params(b)) != HS_OK) return fail(rc);
+  if ((rc = build_plan(b)) != HS_OK) return fail(rc);
+  *out = b;
+  return HS_OK;
+}
+
+int hs_batch_set_params(hs_batch* b, const double* gammas, const double* betas) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  b->gammas.assign(gammas, gammas + size_t(b->ninst) * b->p);
+  b->betas.assign(betas, betas + size_t(b->ninst) * b->p);
+  return upload_params(b);
+}
+
+int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  if (tile_cap < 6 || tile_cap > 12 || ctas_per_sm < 1 || ctas_per_sm > 8)
+    return set_error(HS_E_INVALID, "tile cap 6..12, 1..8 CTAs per SM");
+  const int old_cap = b->tile_cap, old_ctas = b->ctas_per_sm;
+  b->tile_cap = tile_cap;
+  b->ctas_per_sm = ctas_per_sm;
+  std::fill(std::begin(b->cap_of_n), std::end(b->cap_of_n), 0);
+  const int rc = build_plan(b);
+  if (rc != HS_OK) {  // keep the previous schedule usable
+    b->tile_cap = old_cap;
+    b->ctas_per_sm = old_ctas;
+    if (build_plan(b) != HS_OK) return rc;
+  }
+  return rc;
+}
+
+int hs_batch_run(hs_batch* b, double* expect_out, double* ms) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  HS_TRY(run_once(b, ms));
+  if (expect_out) std::memcpy(expect_out, b->h_expect, sizeof(double) * b->ninst);
+  return HS_OK;
+}
+
+int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* best_ms) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  auto timed = [&](double* best) -> int {  // best of two graph replays after a warm one
+    double a = 0, c = 0;
+    HS_TRY(run_once(b, nullptr));
+    HS_TRY(run_once(b, &a));
+    HS_TRY(run_once(b, &c));
+    *best = std::min(a, c);
+    return HS_OK;
+  };
+  // 1) one tile cap for every instance x CTAs per SM
+  double best = 1e300;
+  int bc = b->tile_cap, bt = b->ctas_per_sm;
+  for (int cap : {10, 11, 12})
+    for (int ctas : {2, 4, 6}) {
+      if (hs_batch_configure(b, cap, ctas) != HS_OK) continue;
+      double ms = 0;
+      HS_TRY(timed(&ms));
+      if (ms < best) {
+        best = ms;
+        bc = cap;
+        bt = ctas;
+      }
+    }
+  HS_TRY(hs_batch_configure(b, bc, bt));
+  // 2) per qubit count, largest states first: try the other caps, keep a
+  // change only if the whole batch gets at least 1% faster
+  std::vector<int> ns(b->n.begin(), b->n.end());
+  std::sort(ns.begin(), ns.end());
+  ns.erase(std::unique(ns.begin(), ns.end()), ns.end());
+  std::reverse(ns.begin(), ns.end());
+  for (int n : ns) {
+    if (n <= 10) continue;  // one pass whatever the cap
+    const int keep = b->cap_of_n[n];
+    int chosen = keep;
+    for (int cap : {10, 11, 12}) {
+      if (cap == (keep ? keep : bc)) continue;
+      b->cap_of_n[n] = cap;
+      if (build_plan(b) != HS_OK) continue;
+      double ms = 0;
+      HS_TRY(timed(&ms));
+      if (ms < 0.99 * best) {
+        best = ms;
+        chosen = cap;
+      }
+    }
+    b->cap_of_n[n] = chosen;
+  }
+  HS_TRY(build_plan(b));
+  if (best_cap) *best_cap = bc;
+  if (best_ctas) *best_ctas = bt;
+  if (best_ms) *best_ms = best;
+  return HS_OK;
+}
+
+int hs_batch_tile_caps(hs_batch* b, int32_t* caps) {
+  if (!b || !caps) return set_error(HS_E_INVALID, "null argument");
+  for (int i = 0; i < b->ninst; ++i)
+    caps[i] = b->cap_of_n[b->n[i]] ? b->cap_of_n[b->n[i]] : b->tile_cap;
+  return HS_OK;
+}
+
+int hs_batch_stats(hs_batch* b, int64_t* stats) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  stats[0] = int64_t(b->total);
+  stats[1] = int64_t(b->ncounters);
+  stats[2] = int64_t(b->pass_bytes);
+  stats[3] = b->tile_cap;
+  stats[4] = b->ctas_per_sm;
+  return HS_OK;
+}
+
+int hs_batch_state(hs_batch* b, int instance, void* host_out) {
+  if (!b || instance < 0 || instance >= b->ninst) return set_error(HS_E_INVALID, "bad instance");
+  HS_CUDA(cudaMemcpy(host_out, static_cast<float2*>(b->pool) + b->offset[instance],
+                     sizeof(float2) << b->n[instance], cudaMemcpyDeviceToHost));
+  return HS_OK;
+}
+
+int hs_batch_destroy(hs_batch* b) {
+  if (!b) return HS_OK;
+  free_plan(b);
+  for (void* p : {b->pool, (void*)b->d_par, (void*)b->d_head, (void*)b->d_err, (void*)b->d_expect})
+    if (p) cudaFree(p);
+  if (b->h_expect) cudaFreeHost(b->h_expect);
+  if (b->h_err) cudaFreeHost(b->h_err);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return HS_OK;
+}
+
+}  // extern "C"

@@ -123,6 +123,7 @@ static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
 // state pass).  Returns HS_OK or an error.
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
               int tile_bits_hint, int dtype, std::vector<PartProgram>* programs);
+int current_tile_hint();  // hs_set_tile_qubits' value
 inline int max_tile_bits(int dtype) { (void)dtype; return 12; }
 
 // ---- K2 bit-swap program ----------------------------------------------------
@@ -172,6 +173,51 @@ int reduce_compare(const void* a, int adtype, const void* b, int bdtype, int n, 
 int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, uint64_t count,
                          double out[4], cudaStream_t s);
 
+// ---- batching form (kernels_batch.cu, batch_api.cpp) -------------------------
+constexpr int kBatchMaxQubits = 30;
+constexpr int kBatchMaxEdges = 64;
+constexpr int kBatchMaxRounds = 8;
+constexpr int kBatchMaxPasses = 4;   // passes per round (tile <= 12 bits, 9 new qubits each)
+constexpr int kBatchThreads = 256;
+
+// one pass of a QAOA round over an instance: the tile bits, which of them get
+// the mixer RX, in register groups of 4 (tile-bit positions)
+struct BatchPass {
+  int32_t m;                 // tile bits
+  int32_t ngroups;
+  Runs tile, outer;
+  uint8_t tile_slot[16];
+  uint8_t group_bits[3][4];  // tile bits in registers per group (4 each)
+  uint8_t group_rx[3];       // bit j set: register bit j of the group gets RX
+  uint8_t phase;             // 1: the cost phase is applied in group 0
+};
+
+struct BatchInstance {
+  float2* amp;
+  int32_t n, nedges, p, npasses;
+  uint8_t edge_a[kBatchMaxEdges], edge_b[kBatchMaxEdges];
+  BatchPass pass[kBatchMaxPasses];
+  uint64_t step_base;        // index of this instance's first counter
+};
+
+struct BatchParams {         // per instance per round (updated for sweeps)
+  float2 rx[kBatchMaxRounds][2];        // cos(beta), -i sin(beta) as (c, s)
+  float2 phase[kBatchMaxRounds][kBatchMaxEdges + 1];  // e^{i gamma/2 (2c - |E|)} for cut c
+};
+
+struct BatchItem {           // a contiguous range of work items: one (instance, step)
+  uint64_t first;            // first global item index
+  int32_t inst, step;
+  uint32_t ntiles;
+};
+
+int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
+                 int nitems_groups, uint64_t total_items, uint32_t* d_counters,
+                 unsigned long long* d_head, int* d_err, int grid, cudaStream_t s);
+int launch_batch_init(const BatchInstance* d_inst, int ninst, cudaStream_t s);
+int launch_batch_expect(const BatchInstance* d_inst, int ninst, int max_n, double* d_partial,
+                        double* d_out, cudaStream_t s);
+
 // ---- launchers (kernels_*.cu) ----------------------------------------------
 int launch_part(void* amp, int dtype, const PartProgram& prog, cudaStream_t s);
 int launch_permute(void* amp, int dtype, int n, const int32_t* pairs, int npairs,
@@ -201,6 +247,28 @@ struct TimedRegion {
 };
 
 inline size_t amp_bytes(int dtype) { return dtype == HS_DTYPE_C64 ? 8 : 16; }
+
+// ---- learned cost model (kernels_mlp.cu, mlp_api.cpp) -------------------------
+// in -> 64 -> 64 -> 64 -> 1, ReLU, FP32.  Flat parameter layout (row-major,
+// W[out][in]): W1 b1 W2 b2 W3 b3 W4 b4.
+constexpr int kMlpHidden = 64;
+constexpr int kMlpMaxIn = 64;
+constexpr int kMlpSamples = 64;  // samples per block iteration
+inline int mlp_num_params(int in) {
+  const int H = kMlpHidden;
+  return H * in + H + 2 * (H * H + H) + H + 1;
+}
+int launch_mlp_forward(const float* params, int in, const float* x, int n, float* out,
+                       cudaStream_t s);
+// per-block gradient partials of loss = sum_i scale/2 * (f(x_i) - y_i)^2 over the
+// rows idx[0..n) (idx may be null: rows 0..n); partial: nblk x P, loss_partial: nblk
+int launch_mlp_backward(const float* params, int in, const float* x, const float* y,
+                        const int32_t* idx, int n, float scale, float* partial,
+                        float* loss_partial, int nblk, cudaStream_t s);
+int launch_mlp_reduce(const float* partial, const float* loss_partial, int nblk, int P,
+                      float* grad, float* loss, cudaStream_t s);
+int launch_mlp_adam(float* params, const float* grad, float* m, float* v, int P, float lr,
+                    float beta1, float beta2, float eps, int step, cudaStream_t s);
 
 }  // namespace hisv
 

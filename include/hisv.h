@@ -169,6 +169,12 @@ int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets
 /* Host-only: plan one part (identity slot map) without touching a device and
  * report stats[0..5] = {passes, register groups, ops, dense ops, diagonal
  * ops, tile bits}.  Used by the cost model and by tests of the planner. */
+/* hs_parts_run with every part planned first and then launched back to back,
+ * part_ms[p] = device time of part p (CUDA events between consecutive parts;
+ * synchronises).  The harvest of part timings for the cost model. */
+int hs_parts_run_timed(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
+                       int num_parts, float* part_ms, void* stream);
+
 int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates,
                   int32_t* stats);
 
@@ -241,6 +247,80 @@ int hs_expect_zz(hs_state* st, const int32_t* pairs, int num_pairs, double* out)
  * generator: out[s*nq + j] = value of qubits[j] in sample s. */
 int hs_measure(hs_state* st, const int32_t* qubits, int num_qubits,
                uint32_t num_samples, uint64_t seed, int32_t* out);
+
+/* ---- batching form (no counterpart in the reference) -----------------------
+ * Many QAOA MaxCut circuits of different qubit counts (parameter sweeps), all
+ * advanced by one persistent launch (K6) replayed as a captured CUDA graph:
+ * |+>^n, then p rounds of RZZ(gamma_r) on every edge and RX(2 beta_r) on every
+ * qubit (the reference's RZZ/RX, basic_gates.hpp:341-363,1235-1313), complex64
+ * states, and <H_C> = sum_E (1 - <Z_a Z_b>)/2 per instance accumulated in FP64.
+ * edges: pairs, instance i uses pairs [edge_offsets[i], edge_offsets[i+1]);
+ * gammas / betas: num_instances x p. */
+typedef struct hs_batch hs_batch;
+int hs_batch_create_qaoa(int num_instances, const int32_t* num_qubits,
+                         const int32_t* edge_offsets, const int32_t* edges, int p,
+                         const double* gammas, const double* betas, hs_batch** out);
+/* New angles for the next run (the captured graph is reused). */
+int hs_batch_set_params(hs_batch* b, const double* gammas, const double* betas);
+/* Tile cap (6..12 qubits per pass) and persistent CTAs per SM. */
+int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm);
+/* Autotuner: times every (tile cap, CTAs per SM) candidate on the whole batch
+ * and keeps the best, then refines the tile cap per qubit count (largest
+ * states first), keeping a change only when the batch gets >= 1% faster. */
+int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* best_ms);
+/* The tile cap in force for every instance (num_instances entries). */
+int hs_batch_tile_caps(hs_batch* b, int32_t* caps);
+/* One whole run (graph launch, synchronised): expect_out[i] = <H_C> of
+ * instance i; *ms = device time of the run between CUDA events on the
+ * batch's stream, read-back of the results included (may be NULL). */
+int hs_batch_run(hs_batch* b, double* expect_out, double* ms);
+/* {work items, steps, bytes moved per run, tile cap, CTAs per SM} */
+int hs_batch_stats(hs_batch* b, int64_t* stats);
+/* Complex64 amplitudes of one instance (qubit order) into host memory. */
+int hs_batch_state(hs_batch* b, int instance, void* host_out);
+int hs_batch_destroy(hs_batch* b);
+
+/* ---- learned cost model (no counterpart in the reference) -------------------
+ * A small MLP (in_dim -> 64 -> 64 -> 64 -> 1, ReLU, FP32) that predicts the
+ * log run time of a part from its features; trained on part timings the
+ * simulator measures.  Forward, backward and Adam are the library's own K7
+ * kernels.  Arrays are host memory, x row-major n x in_dim.  Parameters are
+ * one flat array: W1 (64 x in_dim, row-major, W[out][in]) b1 W2 b2 W3 b3 W4 b4. */
+typedef struct hs_mlp hs_mlp;
+int hs_mlp_create(int in_dim, uint64_t seed, hs_mlp** out);
+int hs_mlp_num_params(const hs_mlp* m);
+int hs_mlp_get_params(hs_mlp* m, float* host);
+/* Sets the parameters and resets the Adam moments. */
+int hs_mlp_set_params(hs_mlp* m, const float* host);
+int hs_mlp_predict(hs_mlp* m, const float* x, int n, float* y_out);
+/* Gradient of the mean squared error (1/n) sum (f(x_i) - y_i)^2 with respect
+ * to every parameter, and that loss. */
+int hs_mlp_gradients(hs_mlp* m, const float* x, const float* y, int n, float* grad_out,
+                     float* loss_out);
+/* Minibatch Adam (beta 0.9 / 0.999, eps 1e-8) on the mean squared error,
+ * seeded shuffles; epoch_loss (epochs entries, may be NULL) gets each epoch's
+ * mean squared error. */
+int hs_mlp_train(hs_mlp* m, const float* x, const float* y, int n, int epochs, int batch,
+                 float lr, uint64_t seed, float* epoch_loss);
+int hs_mlp_destroy(hs_mlp* m);
+
+/* Features of parts for the cost model (host only, no GPU): 43 floats per
+ * part = {n/32, part qubits/12, gates/32, non-diagonal target qubits/12,
+ * qubits at slot >= 10 /12, max slot/n, min non-diagonal target slot/n,
+ * fraction of multi-qubit gates, controlled gates/32, the K1 planner's
+ * passes/4, register groups/16, ops/64, dense ops/64, diagonal ops/64, tile
+ * bits/12, then the count/16 of each gate type I..SDG}.  Parts are gate index
+ * lists: part p = part_gates[part_offsets[p] .. part_offsets[p+1]). */
+int hs_num_part_features(void);
+int hs_part_features(int num_qubits, int dtype, const hs_gate* gates, int num_gates,
+                     const int32_t* part_gates, const int32_t* part_offsets, int num_parts,
+                     float* feats);
+/* Every contiguous segment order[i..i+len) with at most max_qubits qubits and
+ * max_len gates (a segment of a topological order is a valid acyclic part),
+ * with its features; *count = number of segments (an error if above capacity). */
+int hs_order_segments(int num_qubits, int dtype, const hs_gate* gates, int num_gates,
+                      const int32_t* order, int max_qubits, int max_len, int capacity,
+                      int32_t* seg_start, int32_t* seg_len, float* feats, int32_t* count);
 
 /* ---- timers (py_wrapper.cpp:163-169) -------------------------------------- */
 /* Accumulated device time of K1/K2 launches in microseconds, and the number of

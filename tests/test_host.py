@@ -132,3 +132,88 @@ def test_records_roundtrip():
     assert r["type"].tolist() == [25, 19]
     assert r["controls"][0][:2].tolist() == [1, 2]
     assert r["frac_num"][1] == 3 and r["frac_pow"][1] == 4
+
+
+def test_odd_qubit_counts_use_near_regular_graphs():
+    for n in (17, 21, 25):
+        edges = circuits.random_maxcut_graph(n, np.random.default_rng(n))
+        deg = np.bincount(np.array(edges).reshape(-1), minlength=n)
+        assert sorted(deg.tolist()) == [2] + [3] * (n - 1)
+        assert len(edges) == (3 * n - 1) // 2
+    assert len(circuits.random_maxcut_graph(16, np.random.default_rng(0))) == 24
+
+
+@pytest.mark.parametrize("bad", ["small_n", "big_n", "self_loop", "edge_range", "rounds"])
+def test_batch_rejects_bad_instances(bad):
+    n, edges, p = 8, [(0, 1), (2, 3)], 2
+    if bad == "small_n":
+        n = 3
+        edges = [(0, 1)]
+    elif bad == "big_n":
+        n = 31
+    elif bad == "self_loop":
+        edges = [(2, 2)]
+    elif bad == "edge_range":
+        edges = [(0, 8)]
+    elif bad == "rounds":
+        p = 9
+    with pytest.raises(abi.HisvError) as e:
+        abi.QaoaBatch([(n, edges, [0.1] * p, [0.2] * p)], p)
+    assert e.value.code == abi.HS_E_INVALID
+
+
+class _PassCountModel:
+    """Stand-in cost model (no GPU): one unit per K1 pass plus a little per gate."""
+
+    trained = True
+
+    def predict_ms(self, X, n):
+        return X[:, 9] * 4.0 + X[:, 2] * 0.05
+
+
+def test_part_features_layout():
+    from hisvsim_b200 import learned  # noqa: F401  (imports without a GPU)
+
+    gates = circuits.random_u3_cz(12, 4, 2)
+    parts = partition.partition_acyclic(gates, 5)
+    f = abi.part_features(12, gates, parts)
+    assert f.shape == (len(parts), abi.num_part_features()) == (len(parts), 43)
+    assert np.all(f[:, 0] == np.float32(12 / 32))
+    for p, row in zip(parts, f):
+        assert row[2] == pytest.approx(len(p) / 32)
+        qs = {q for i in p for q in gates[i].controls + gates[i].targets}
+        assert row[1] == pytest.approx(len(qs) / 12)
+        st = abi.plan_stats(12, [gates[i] for i in p], abi.C64)
+        assert row[9] == pytest.approx(st["passes"] / 4) and row[14] == pytest.approx(st["tile_bits"] / 12)
+        assert row[15:].sum() == pytest.approx(len(p) / 16)
+
+
+def test_order_segments_are_convex_parts():
+    gates = circuits.random_layered(10, 5, 4)
+    order = partition.dfs_order(gates)
+    st, ln, ft = abi.order_segments(10, gates, order, 6, 20)
+    assert len(st) == len(ln) == len(ft) > 0
+    assert (ln >= 1).all() and (ln <= 20).all()
+    for a, l in list(zip(st, ln))[::37]:
+        seg = [order[i] for i in range(a, a + l)]
+        qs = {q for i in seg for q in gates[i].controls + gates[i].targets}
+        assert len(qs) <= 6
+    rc = abi.lib().hs_order_segments(10, 1, None, 0, None, 6, 20, 0, None, None, None, None)
+    assert rc == abi.HS_E_INVALID
+
+
+def test_proposer_dp_and_fallback():
+    from hisvsim_b200 import learned
+
+    gates = circuits.random_u3_cz(14, 6, 9)
+    fb = learned.propose(gates, 14, None, default_k=7)
+    assert fb["method"].startswith("acyclic k=7")
+    assert fb["parts"] == partition.partition_acyclic(gates, 7)
+    prop = learned.propose(gates, 14, _PassCountModel(), ks=(5, 7, 9))
+    assert partition.is_valid_partition(gates, prop["parts"])
+    best_acyclic = min(v for k, v in prop["candidates"].items() if k.startswith("acyclic"))
+    assert prop["predicted_ms"] <= best_acyclic + 1e-9
+    # the dynamic program is exact: no segmentation of its order is cheaper
+    cuts, total = learned._dp(np.array([0, 0, 1, 2]), np.array([1, 3, 2, 1]),
+                              np.array([1.0, 2.5, 1.0, 1.0]), 3)
+    assert cuts == [(0, 1), (1, 2)] and total == 2.0

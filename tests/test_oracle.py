@@ -134,3 +134,38 @@ def test_gather_slots_semantics(port):
 def test_reference_rejects_alloc(ref):
     with pytest.raises(ValueError):
         ref.run(2, to_records([Gate("ALLOC", (0,))]))
+
+
+# ---- the cost model's network (oracle/mlp.py), pinned by finite differences
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle import mlp
+
+    rng = np.random.default_rng(3)
+    d = 7
+    p = rng.normal(0, 0.3, mlp.num_params(d))
+    x = rng.normal(0, 1, (19, d))
+    y = rng.normal(0, 1, 19)
+    loss, g = mlp.loss_and_grad(p, x, y)
+    idx = rng.choice(p.size, 60, replace=False)
+    idx = np.concatenate([idx, [p.size - 1, mlp.num_params(d) - 65]])  # b4 and a w4 entry
+    h = 1e-6
+    for i in idx:
+        e = np.zeros_like(p)
+        e[i] = h
+        fd = (mlp.loss_and_grad(p + e, x, y)[0] - mlp.loss_and_grad(p - e, x, y)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])
+    assert loss == pytest.approx(np.mean((mlp.forward(p, x)[0] - y) ** 2))
+
+
+def test_mlp_oracle_adam_known_step():
+    from oracle import mlp
+
+    p = np.array([1.0, -2.0, 0.5])
+    g = np.array([0.1, -0.3, 0.0])
+    m = np.zeros(3)
+    v = np.zeros(3)
+    mlp.adam_step(p, g, m, v, 1, 0.01)
+    # first bias-corrected step moves each coordinate by lr * sign(g) (g != 0)
+    assert p == pytest.approx([0.99, -1.99, 0.5], abs=1e-7)
