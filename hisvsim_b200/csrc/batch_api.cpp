@@ -15,7 +15,7 @@ struct hs_batch {
   std::vector<int> n;
   std::vector<std::vector<std::pair<int, int>>> edges;
   std::vector<double> gammas, betas;
-  int tile_cap = 12, ctas_per_sm = 4;
+  int tile_cap = 12, ctas_per_sm = 3, chunk = 8;
   int cap_of_n[kBatchMaxQubits + 1] = {};  // per qubit count; 0 = tile_cap
   void* pool = nullptr;
   std::vector<uint64_t> offset;  // amplitude offset of each instance in the pool
@@ -23,6 +23,7 @@ struct hs_batch {
   BatchParams* d_par = nullptr;
   BatchItem* d_items = nullptr;
   uint32_t* d_counters = nullptr;
+  uint8_t* d_cut = nullptr;
   unsigned long long* d_head = nullptr;
   int* d_err = nullptr;
   double* d_partial = nullptr;
@@ -44,8 +45,10 @@ void free_plan(hs_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
-  for (void* p : {(void*)b->d_inst, (void*)b->d_items, (void*)b->d_counters, (void*)b->d_partial})
+  for (void* p : {(void*)b->d_inst, (void*)b->d_items, (void*)b->d_counters, (void*)b->d_partial,
+                  (void*)b->d_cut})
     if (p) cudaFree(p);
+  b->d_cut = nullptr;
   b->d_inst = nullptr;
   b->d_items = nullptr;
   b->d_counters = nullptr;
@@ -146,6 +149,18 @@ int upload_params(hs_batch* b) {
   return HS_OK;
 }
 
+// cut of the edges with both ends in qubits [0, m), for every x < 2^m
+void cut_low_table(const std::vector<std::pair<int, int>>& edges, int m, uint8_t* out) {
+  std::vector<std::pair<int, int>> in;
+  for (const auto& e : edges)
+    if (e.first < m && e.second < m) in.push_back(e);
+  for (uint32_t x = 0; x < (1u << m); ++x) {
+    int c = 0;
+    for (const auto& e : in) c += int(((x >> e.first) ^ (x >> e.second)) & 1u);
+    out[x] = uint8_t(c);
+  }
+}
+
 int build_plan(hs_batch* b) {
   free_plan(b);
   std::vector<BatchInstance> inst(b->ninst);
@@ -153,6 +168,8 @@ int build_plan(hs_batch* b) {
   uint64_t nc = 0;
   int maxsteps = 0;
   b->pass_bytes = 0;
+  std::vector<size_t> cut_off(b->ninst);
+  size_t cut_bytes = 0;
   for (int i = 0; i < b->ninst; ++i) {
     BatchInstance& I = inst[i];
     I.amp = static_cast<float2*>(b->pool) + b->offset[i];
@@ -168,9 +185,19 @@ int build_plan(hs_batch* b) {
     const int steps = I.npasses * b->p;
     nc += uint64_t(steps);
     maxsteps = std::max(maxsteps, steps);
-    b->pass_bytes += uint64_t(steps) * 2ull * (8ull << I.n);
+    for (int k = 0; k < steps; ++k) b->pass_bytes += 2ull * (8ull << I.n);
+    cut_off[i] = cut_bytes;
+    cut_bytes += size_t(1) << I.pass[0].m;
   }
+  std::vector<uint8_t> cut(cut_bytes);
+  for (int i = 0; i < b->ninst; ++i)
+    cut_low_table(b->edges[i], inst[i].pass[0].m, cut.data() + cut_off[i]);
+  HS_CUDA(cudaMalloc(&b->d_cut, cut_bytes));
+  HS_CUDA(cudaMemcpy(b->d_cut, cut.data(), cut_bytes, cudaMemcpyHostToDevice));
+  for (int i = 0; i < b->ninst; ++i) inst[i].cut_low = b->d_cut + cut_off[i];
+  // work items: per step level, per instance, the step's tiles in chunks
   std::vector<BatchItem> items;
+  std::vector<uint32_t> prev_chunks(b->ninst, 0);
   uint64_t total = 0;
   for (int k = 0; k < maxsteps; ++k)
     for (int i = 0; i < b->ninst; ++i) {
@@ -181,17 +208,20 @@ int build_plan(hs_batch* b) {
       it.inst = i;
       it.step = k;
       it.ntiles = uint32_t(1ull << (I.n - I.pass[k % I.npasses].m));
+      it.chunk = std::min<uint32_t>(uint32_t(b->chunk), it.ntiles);
+      it.need = prev_chunks[i];
+      const uint32_t nchunks = (it.ntiles + it.chunk - 1) / it.chunk;
+      prev_chunks[i] = nchunks;
       items.push_back(it);
-      total += it.ntiles;
+      total += nchunks;
     }
   b->ngroups = int(items.size());
   b->total = total;
   b->ncounters = nc;
-  const int max_chunks = 1 << (b->max_n > 16 ? b->max_n - 16 : 0);
   HS_CUDA(cudaMalloc(&b->d_inst, sizeof(BatchInstance) * inst.size()));
   HS_CUDA(cudaMalloc(&b->d_items, sizeof(BatchItem) * items.size()));
   HS_CUDA(cudaMalloc(&b->d_counters, sizeof(uint32_t) * nc));
-  HS_CUDA(cudaMalloc(&b->d_partial, sizeof(double) * size_t(b->ninst) * max_chunks));
+  HS_CUDA(cudaMalloc(&b->d_partial, sizeof(double) * size_t(b->ninst) * 256));
   HS_CUDA(cudaMemcpy(b->d_inst, inst.data(), sizeof(BatchInstance) * inst.size(),
                      cudaMemcpyHostToDevice));
   HS_CUDA(cudaMemcpy(b->d_items, items.data(), sizeof(BatchItem) * items.size(),
@@ -208,7 +238,8 @@ int build_plan(hs_batch* b) {
   int rc = launch_batch_init(b->d_inst, b->ninst, b->stream);
   if (rc == HS_OK)
     rc = launch_batch(b->d_inst, b->d_par, b->d_items, b->ngroups, b->total, b->d_counters,
-                      b->d_head, b->d_err, sms * b->ctas_per_sm, b->stream);
+                      b->d_head, b->d_err,
+                      sms * std::min(b->ctas_per_sm, batch_max_ctas_per_sm()), b->stream);
   if (rc == HS_OK)
     rc = launch_batch_expect(b->d_inst, b->ninst, b->max_n, b->d_partial, b->d_expect, b->stream);
   cudaMemcpyAsync(b->h_expect, b->d_expect, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost,
@@ -315,6 +346,14 @@ int hs_batch_set_params(hs_batch* b, const double* gammas, const double* betas) 
   return upload_params(b);
 }
 
+int hs_batch_set_chunk(hs_batch* b, int tiles_per_item) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  if (tiles_per_item < 1 || tiles_per_item > 4096)
+    return set_error(HS_E_INVALID, "tiles per work item 1..4096");
+  b->chunk = tiles_per_item;
+  return build_plan(b);
+}
+
 int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm) {
   if (!b) return set_error(HS_E_INVALID, "null batch");
   if (tile_cap < 6 || tile_cap > 12 || ctas_per_sm < 1 || ctas_per_sm > 8)
@@ -349,20 +388,26 @@ int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* be
     *best = std::min(a, c);
     return HS_OK;
   };
-  // 1) one tile cap for every instance x CTAs per SM
+  // 1) one tile cap for every instance x CTAs per SM (up to the occupancy
+  // limit) x tiles per work item
   double best = 1e300;
-  int bc = b->tile_cap, bt = b->ctas_per_sm;
+  const int maxc = batch_max_ctas_per_sm();
+  int bc = b->tile_cap, bt = b->ctas_per_sm, bk = b->chunk;
   for (int cap : {10, 11, 12})
-    for (int ctas : {2, 4, 6}) {
-      if (hs_batch_configure(b, cap, ctas) != HS_OK) continue;
-      double ms = 0;
-      HS_TRY(timed(&ms));
-      if (ms < best) {
-        best = ms;
-        bc = cap;
-        bt = ctas;
+    for (int ctas : {std::max(1, maxc - 1), maxc})
+      for (int chunk : {4, 16}) {
+        b->chunk = chunk;
+        if (hs_batch_configure(b, cap, ctas) != HS_OK) continue;
+        double ms = 0;
+        HS_TRY(timed(&ms));
+        if (ms < best) {
+          best = ms;
+          bc = cap;
+          bt = ctas;
+          bk = chunk;
+        }
       }
-    }
+  b->chunk = bk;
   HS_TRY(hs_batch_configure(b, bc, bt));
   // 2) per qubit count, largest states first: try the other caps, keep a
   // change only if the whole batch gets at least 1% faster
@@ -407,7 +452,8 @@ int hs_batch_stats(hs_batch* b, int64_t* stats) {
   stats[1] = int64_t(b->ncounters);
   stats[2] = int64_t(b->pass_bytes);
   stats[3] = b->tile_cap;
-  stats[4] = b->ctas_per_sm;
+  stats[4] = std::min(b->ctas_per_sm, batch_max_ctas_per_sm());
+  stats[5] = b->chunk;
   return HS_OK;
 }
 

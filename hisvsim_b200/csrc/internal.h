@@ -198,6 +198,7 @@ struct BatchInstance {
   uint8_t edge_a[kBatchMaxEdges], edge_b[kBatchMaxEdges];
   BatchPass pass[kBatchMaxPasses];
   uint64_t step_base;        // index of this instance's first counter
+  const uint8_t* cut_low;    // 2^pass[0].m entries: cut of the edges inside qubits [0, m)
 };
 
 struct BatchParams {         // per instance per round (updated for sweeps)
@@ -205,15 +206,17 @@ struct BatchParams {         // per instance per round (updated for sweeps)
   float2 phase[kBatchMaxRounds][kBatchMaxEdges + 1];  // e^{i gamma/2 (2c - |E|)} for cut c
 };
 
-struct BatchItem {           // a contiguous range of work items: one (instance, step)
-  uint64_t first;            // first global item index
+struct BatchItem {           // one (instance, step): its tiles in chunks, one work item per chunk
+  uint64_t first;            // global index of the first chunk
   int32_t inst, step;
-  uint32_t ntiles;
+  uint32_t ntiles, chunk;    // tiles of the step, tiles per chunk
+  uint32_t need;             // chunks of the previous step of this instance
 };
 
 int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
                  int nitems_groups, uint64_t total_items, uint32_t* d_counters,
                  unsigned long long* d_head, int* d_err, int grid, cudaStream_t s);
+int batch_max_ctas_per_sm();  // occupancy limit of the persistent kernel
 int launch_batch_init(const BatchInstance* d_inst, int ninst, cudaStream_t s);
 int launch_batch_expect(const BatchInstance* d_inst, int ninst, int max_n, double* d_partial,
                         double* d_out, cudaStream_t s);

@@ -1,16 +1,27 @@
 // K6: the batching form.  Many QAOA MaxCut instances of different qubit counts
-// are advanced by ONE persistent launch: CTAs take work items (instance, step,
-// tile) from a global queue in step order; a step of an instance is one pass
-// over its complex64 state (the first pass of a round applies the cost phase
+// are advanced by ONE persistent launch.  A step of an instance is one pass
+// over its complex64 state: the first pass of a round applies the cost phase
 // e^{i gamma/2 (2 cut(x) - |E|)} = prod_E RZZ(gamma), every pass applies the
-// mixer RX(2 beta) to its share of the qubits).  A tile of step k waits for all
-// tiles of step k-1 of the same instance through a completion counter; items
-// are dequeued in step order, so the earliest unfinished item never waits and
+// mixer RX(2 beta) to its share of the qubits.  The tiles of a step are cut
+// into chunks; CTAs take chunks from a global queue in step order and stream
+// their tiles through two shared-memory buffers (the next tile loads while
+// the current one is processed).  A chunk of step k waits until every chunk
+// of step k-1 of its instance is done (a completion counter); chunks are
+// dequeued in step order, so the earliest unfinished chunk never waits and
 // the queue always drains.  Waits are bounded: a timeout sets an error flag.
+//
+// cut(x) in the phase pass: the tile holds qubits [0, m), so with the outer
+// bits fixed, cut(x) = cut_low[i] + C + sum_q w_q i_q, where cut_low counts
+// the edges inside [0, m) (a per-instance table), C the edges outside it plus
+// the crossing edges whose outer end is 1, and w_q = (#crossing edges of q
+// whose outer end is 0) - (#those whose outer end is 1).
 #include "internal.h"
 
 namespace hisv {
 namespace {
+
+constexpr int kTileMax = 4096;
+constexpr uint32_t kDepLimit = 1u << 24;  // polls (with ~0.1 us sleeps) before giving up
 
 __device__ __forceinline__ uint64_t bdep(uint64_t x, const Runs& r) {
   uint64_t out = 0;
@@ -26,187 +37,215 @@ __device__ __forceinline__ uint32_t bswz(uint32_t i) {
 __device__ __forceinline__ void cp16(uint32_t saddr, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
 }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
-// cut(x) = number of edges whose endpoints differ in x
-__device__ __forceinline__ int cut_full(uint64_t x, const BatchInstance& I) {
+struct Shared {
+  float2 phase[kBatchMaxEdges + 1];
+  uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
+  uint8_t cut[kTileMax];
+  int w[16];
+  int c;
+  int group;
+  int abort;
+  unsigned long long item;
+};
+
+// w_q and C of the tile whose outer bits are gbase (warp 0 only)
+__device__ __forceinline__ void cross_weights(Shared& S, int nedges, int m, uint64_t gbase) {
+  const int lane = threadIdx.x & 31;
+  if (lane < 16) S.w[lane] = 0;
+  __syncwarp();
   int c = 0;
-  for (int e = 0; e < I.nedges; ++e) c += int(((x >> I.edge_a[e]) ^ (x >> I.edge_b[e])) & 1ull);
-  return c;
-}
-
-// cut(xb | S) for the 16 subsets S of four qubits q[0..3] (all 0 in xb):
-// edges with exactly one endpoint among q flip when that endpoint is set,
-// edges between two of them flip when exactly one of the two is set
-__device__ __forceinline__ void cut_table(uint64_t xb, const uint8_t (&q)[4], const BatchInstance& I,
-                                          int (&out)[16]) {
-  int d[4] = {0, 0, 0, 0};
-  int rr[6];
-  int nrr = 0;
-  int c0 = 0;
-  for (int e = 0; e < I.nedges; ++e) {
-    const int a = I.edge_a[e], b = I.edge_b[e];
-    const int ba = int((xb >> a) & 1ull), bb = int((xb >> b) & 1ull);
-    c0 += ba ^ bb;
-    int ja = -1, jb = -1;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (q[j] == a) ja = j;
-      if (q[j] == b) jb = j;
-    }
-    if (ja >= 0 && jb >= 0) {
-      if (nrr < 6) rr[nrr++] = (1 << ja) | (1 << jb);
-    } else if (ja >= 0) {
-      d[ja] += 1 - 2 * (ba ^ bb);
-    } else if (jb >= 0) {
-      d[jb] += 1 - 2 * (ba ^ bb);
+  for (int e = lane; e < nedges; e += 32) {
+    const int a = S.ea[e], b = S.eb[e];
+    const int xa = int((gbase >> a) & 1ull), xb = int((gbase >> b) & 1ull);
+    const bool la = a < m, lb = b < m;
+    if (!la && !lb) {
+      c += xa ^ xb;
+    } else if (la && !lb) {
+      c += xb;
+      atomicAdd(&S.w[a], xb ? -1 : 1);
+    } else if (!la && lb) {
+      c += xa;
+      atomicAdd(&S.w[b], xa ? -1 : 1);
     }
   }
-#pragma unroll
-  for (int S = 0; S < 16; ++S) {
-    int c = c0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if ((S >> j) & 1) c += d[j];
-    for (int k = 0; k < nrr; ++k) {
-      const int w = S & rr[k];
-      c += (w != 0 && w != rr[k]) ? 1 : 0;
-    }
-    out[S] = c;
-  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (lane == 0) S.c = c;
 }
-
-constexpr uint32_t kDepLimit = 1u << 24;  // polls (with ~0.1 us sleeps) before giving up
 
 __global__ void __launch_bounds__(kBatchThreads, 3)
     k6_batch(const BatchInstance* __restrict__ insts, const BatchParams* __restrict__ pars,
              const BatchItem* __restrict__ groups, int ngroups, uint64_t total,
              uint32_t* __restrict__ counters, unsigned long long* __restrict__ head,
              int* __restrict__ err) {
-  __shared__ __align__(16) float2 tile[4096];
-  __shared__ float2 s_phase[kBatchMaxEdges + 1];
-  __shared__ unsigned long long s_item;
-  __shared__ int s_abort;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tiles = reinterpret_cast<float2*>(smem_raw);  // two buffers of kTileMax
+  Shared& S = *reinterpret_cast<Shared*>(smem_raw + 2 * kTileMax * sizeof(float2));
   const int t = threadIdx.x;
-  const uint32_t tile_s = uint32_t(__cvta_generic_to_shared(tile));
+  const uint32_t tiles_s = uint32_t(__cvta_generic_to_shared(tiles));
   for (;;) {
-    if (t == 0) s_item = atomicAdd(head, 1ull);
-    __syncthreads();
-    const uint64_t item = s_item;
-    if (item >= total) break;
-    // the item's (instance, step) group: last group with first <= item
-    int lo = 0, hi = ngroups - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (groups[mid].first <= item) lo = mid; else hi = mid - 1;
+    if (t == 0) {
+      const unsigned long long item = atomicAdd(head, 1ull);
+      S.item = item;
+      S.abort = 0;
+      if (item < total) {
+        // the item's (instance, step) group: last group with first <= item
+        int lo = 0, hi = ngroups - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (groups[mid].first <= item) lo = mid; else hi = mid - 1;
+        }
+        S.group = lo;
+        const BatchItem& G = groups[lo];
+        if (G.step > 0) {  // every chunk of the previous step of this instance
+          const uint32_t* cnt = counters + insts[G.inst].step_base + (G.step - 1);
+          uint32_t polls = 0, seen;
+          do {
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(cnt) : "memory");
+            if (seen >= G.need) break;
+            __nanosleep(100);
+          } while (++polls < kDepLimit);
+          if (seen < G.need) {
+            S.abort = 1;
+            atomicExch(err, 1);
+          }
+        }
+      }
     }
-    const BatchItem G = groups[lo];
+    __syncthreads();
+    const unsigned long long item = S.item;
+    if (item >= total || S.abort) break;
+    const BatchItem G = groups[S.group];
     const BatchInstance& I = insts[G.inst];
     const int k = G.step;
     const int round = k / I.npasses, pj = k - round * I.npasses;
     const BatchPass& P = I.pass[pj];
-    const uint64_t tix = item - G.first;
-    // dependency on the previous step of this instance
-    if (t == 0) {
-      s_abort = 0;
-      if (k > 0) {
-        const BatchPass& Pp = I.pass[(k - 1) % I.npasses];
-        const uint32_t need = uint32_t(1ull << (I.n - Pp.m));
-        const uint32_t* cnt = counters + I.step_base + (k - 1);
-        uint32_t polls = 0;
-        uint32_t seen;
-        do {
-          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(cnt) : "memory");
-          if (seen >= need) break;
-          __nanosleep(100);
-        } while (++polls < kDepLimit);
-        if (seen < need) {
-          s_abort = 1;
-          atomicExch(err, 1);
-        }
-      }
-    }
-    if (t < kBatchMaxEdges + 1) s_phase[t] = pars[G.inst].phase[round][t];
-    __syncthreads();
-    if (s_abort) break;
-    const int m = P.m, T = 1 << m;
-    const uint64_t gbase = bdep(tix, P.outer);
+    const int m = P.m, T = 1 << m, ngr = P.ngroups, nedges = I.nedges;
+    const bool phase = P.phase != 0;
+    const uint32_t t_begin = uint32_t(item - G.first) * G.chunk;
+    const uint32_t t_end = min(G.ntiles, t_begin + G.chunk);
     float2* amp = I.amp;
-    // load: 16-byte chunks of two amplitudes (tile bit 0 is slot 0)
-    for (int c = t; c < T / 2; c += kBatchThreads)
-      cp16(tile_s + bswz(2u * uint32_t(c)) * 8u, amp + gbase + bdep(2ull * c, P.tile));
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-    __syncthreads();
+    if (phase) {
+      if (t < nedges + 1) S.phase[t] = pars[G.inst].phase[round][t];
+      if (t < nedges) {
+        S.ea[t] = I.edge_a[t];
+        S.eb[t] = I.edge_b[t];
+      }
+      for (int i = t; i < T; i += kBatchThreads) S.cut[i] = I.cut_low[i];
+    }
     const float2 rx = pars[G.inst].rx[round][0];  // (cos beta, sin beta)
     const bool active = t < (T >> 4);
-    for (int g = 0; g < P.ngroups; ++g) {
-      if (active) {
-        // thread bits: the tile bits not held in registers, ascending
-        uint32_t thr = 0;
-        {
-          uint32_t rmask = 0;
-          for (int j = 0; j < 4; ++j) rmask |= 1u << P.group_bits[g][j];
-          int src = 0;
-          for (int b = 0; b < m; ++b)
-            if (!((rmask >> b) & 1u)) thr |= uint32_t((t >> src++) & 1) << b;
-        }
-        uint32_t rb[4];
+    // thread bits of each register group: the tile bits not held in registers
+    uint32_t thr[3] = {0, 0, 0};
+    for (int g = 0; g < ngr; ++g) {
+      uint32_t rmask = 0;
+      for (int j = 0; j < 4; ++j) rmask |= 1u << P.group_bits[g][j];
+      int src = 0;
+      for (int b = 0; b < m; ++b)
+        if (!((rmask >> b) & 1u)) thr[g] |= uint32_t((t >> src++) & 1) << b;
+    }
+    // prologue: first tile into buffer 0
+    {
+      const uint64_t gbase = bdep(t_begin, P.outer);
+      for (int c = t; c < T / 2; c += kBatchThreads)
+        cp16(tiles_s + bswz(2u * uint32_t(c)) * 8u, amp + gbase + bdep(2ull * c, P.tile));
+      cp_commit();
+    }
+    for (uint32_t ti = t_begin; ti < t_end; ++ti) {
+      const int buf = int(ti - t_begin) & 1;
+      float2* tile = tiles + buf * kTileMax;
+      const uint64_t gbase = bdep(ti, P.outer);
+      __syncthreads();  // the other buffer's previous tile is fully stored
+      if (ti + 1 < t_end) {
+        const uint64_t nbase = bdep(ti + 1, P.outer);
+        const uint32_t ns = tiles_s + uint32_t((buf ^ 1) * kTileMax * 8);
+        for (int c = t; c < T / 2; c += kBatchThreads)
+          cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nbase + bdep(2ull * c, P.tile));
+        cp_commit();
+        cp_wait<1>();
+      } else {
+        cp_wait<0>();
+      }
+      if (phase && t < 32) cross_weights(S, nedges, m, gbase);
+      __syncthreads();
+      for (int g = 0; g < ngr; ++g) {
+        if (active) {
+          uint32_t rb[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) rb[j] = 1u << P.group_bits[g][j];
-        float2 v[16];
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          uint32_t idx = thr;
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if ((e >> j) & 1) idx |= rb[j];
-          v[e] = tile[bswz(idx)];
-        }
-        if (g == 0 && P.phase) {
-          uint8_t q[4];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) q[j] = P.tile_slot[P.group_bits[0][j]];
-          int cut[16];
-          cut_table(gbase | bdep(thr, P.tile), q, I, cut);
+          for (int j = 0; j < 4; ++j) rb[j] = 1u << P.group_bits[g][j];
+          float2 v[16];
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
-            const float2 ph = s_phase[cut[e]];
-            const float2 a = v[e];
-            v[e] = make_float2(ph.x * a.x - ph.y * a.y, ph.x * a.y + ph.y * a.x);
+            uint32_t idx = thr[g];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if ((e >> j) & 1) idx |= rb[j];
+            v[e] = tile[bswz(idx)];
+          }
+          if (g == 0 && phase) {
+            // cut = cut_low[i] + C + sum_q w_q i_q (tile bit q is qubit q)
+            int dthr = S.c;
+            for (int b = 0; b < m; ++b)
+              if ((thr[0] >> b) & 1u) dthr += S.w[b];
+            int wr[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) wr[j] = S.w[P.group_bits[0][j]];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              uint32_t idx = thr[0];
+              int cc = dthr;
+#pragma unroll
+              for (int j = 0; j < 4; ++j)
+                if ((e >> j) & 1) {
+                  idx |= rb[j];
+                  cc += wr[j];
+                }
+              const float2 ph = S.phase[int(S.cut[idx]) + cc];
+              const float2 a = v[e];
+              v[e] = make_float2(ph.x * a.x - ph.y * a.y, ph.x * a.y + ph.y * a.x);
+            }
+          }
+          // mixer RX(2 beta) = [[c, -i s], [-i s, c]] on the group's target bits
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (!((P.group_rx[g] >> j) & 1)) continue;
+#pragma unroll
+            for (int e0 = 0; e0 < 16; ++e0) {
+              if ((e0 >> j) & 1) continue;
+              const int e1 = e0 | (1 << j);
+              const float2 a = v[e0], b = v[e1];
+              v[e0] = make_float2(rx.x * a.x + rx.y * b.y, rx.x * a.y - rx.y * b.x);
+              v[e1] = make_float2(rx.y * a.y + rx.x * b.x, -rx.y * a.x + rx.x * b.y);
+            }
+          }
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            uint32_t idx = thr[g];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if ((e >> j) & 1) idx |= rb[j];
+            tile[bswz(idx)] = v[e];
           }
         }
-        // mixer RX(2 beta) = [[c, -i s], [-i s, c]] on the group's target bits
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          if (!((P.group_rx[g] >> j) & 1)) continue;
-#pragma unroll
-          for (int e0 = 0; e0 < 16; ++e0) {
-            if ((e0 >> j) & 1) continue;
-            const int e1 = e0 | (1 << j);
-            const float2 a = v[e0], b = v[e1];
-            v[e0] = make_float2(rx.x * a.x + rx.y * b.y, rx.x * a.y - rx.y * b.x);
-            v[e1] = make_float2(rx.y * a.y + rx.x * b.x, -rx.y * a.x + rx.x * b.y);
-          }
-        }
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          uint32_t idx = thr;
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if ((e >> j) & 1) idx |= rb[j];
-          tile[bswz(idx)] = v[e];
-        }
+        __syncthreads();
       }
-      __syncthreads();
-    }
-    for (int c = t; c < T / 2; c += kBatchThreads) {
-      const uint4 d = *reinterpret_cast<const uint4*>(&tile[bswz(2u * uint32_t(c))]);
-      *reinterpret_cast<uint4*>(amp + gbase + bdep(2ull * c, P.tile)) = d;
+      for (int c = t; c < T / 2; c += kBatchThreads) {
+        const uint4 d = *reinterpret_cast<const uint4*>(&tile[bswz(2u * uint32_t(c))]);
+        *reinterpret_cast<uint4*>(amp + gbase + bdep(2ull * c, P.tile)) = d;
+      }
     }
     __threadfence();
     __syncthreads();
     if (t == 0) atomicAdd(counters + I.step_base + k, 1u);
   }
 }
+
+constexpr size_t kBatchSmem = 2 * kTileMax * sizeof(float2) + sizeof(Shared);
 
 // |+>^n: every amplitude 2^(-n/2)
 __global__ void k6_init(const BatchInstance* __restrict__ insts) {
@@ -218,59 +257,77 @@ __global__ void k6_init(const BatchInstance* __restrict__ insts) {
     I.amp[i] = make_float2(a, 0.f);
 }
 
-// <H_C> = sum_x |a_x|^2 cut(x) in FP64: block (chunk, instance) sums 2^16
-// consecutive amplitudes (16 per thread, cut by table), then one block per
-// instance adds its chunk partials in order
-constexpr int kChunkBits = 16;
+// <H_C> = sum_x |a_x|^2 cut(x) in FP64.  Block (b, instance) takes ranges of
+// 2^m amplitudes (m = the phase pass's tile bits, so cut_low applies) r = b,
+// b + gridDim.x, ...; per range warp 0 derives C and w_q as in K6, then every
+// thread sums its amplitudes.  Per-block partials, added in order by
+// k6_expect_finish: the result does not depend on timing.
+constexpr int kExpectBlocks = 256;
 
 __global__ void __launch_bounds__(256) k6_expect(const BatchInstance* __restrict__ insts,
-                                                 double* __restrict__ partial, int max_chunks) {
+                                                 double* __restrict__ partial) {
+  __shared__ Shared S;
   __shared__ double sh[8];
   const BatchInstance& I = insts[blockIdx.y];
-  const int cb = I.n < kChunkBits ? I.n : kChunkBits;
-  const uint64_t nchunks = 1ull << (I.n - cb);
-  if (blockIdx.x >= nchunks) return;
-  const uint64_t base = uint64_t(blockIdx.x) << cb;
+  const int m = I.pass[0].m, nedges = I.nedges, t = threadIdx.x;
+  const uint64_t nranges = 1ull << (I.n - m);
+  for (int i = t; i < (1 << m); i += 256) S.cut[i] = I.cut_low[i];
+  if (t < nedges) {
+    S.ea[t] = I.edge_a[t];
+    S.eb[t] = I.edge_b[t];
+  }
   double s = 0;
-  const uint8_t q[4] = {0, 1, 2, 3};
-  for (uint64_t i = uint64_t(threadIdx.x) * 16; i < (1ull << cb); i += 256ull * 16) {
-    int cut[16];
-    cut_table(base + i, q, I, cut);
-#pragma unroll
-    for (int e = 0; e < 16; ++e) {
-      const float2 a = I.amp[base + i + e];
-      s += (double(a.x) * a.x + double(a.y) * a.y) * double(cut[e]);
+  for (uint64_t r = blockIdx.x; r < nranges; r += gridDim.x) {
+    __syncthreads();
+    if (t < 32) cross_weights(S, nedges, m, r << m);
+    __syncthreads();
+    const float2* a = I.amp + (r << m);
+    for (int i = t; i < (1 << m); i += 256) {
+      int c = S.c + int(S.cut[i]);
+      for (int b = 0; b < m; ++b)
+        if ((i >> b) & 1) c += S.w[b];
+      const float2 v = a[i];
+      s += (double(v.x) * v.x + double(v.y) * v.y) * double(c);
     }
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  if ((t & 31) == 0) sh[t >> 5] = s;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (t == 0) {
     double r = 0;
     for (int w = 0; w < 8; ++w) r += sh[w];
-    partial[size_t(blockIdx.y) * max_chunks + blockIdx.x] = r;
+    partial[size_t(blockIdx.y) * kExpectBlocks + blockIdx.x] = r;
   }
 }
 
-__global__ void k6_expect_finish(const BatchInstance* __restrict__ insts,
-                                 const double* __restrict__ partial, int max_chunks,
-                                 double* __restrict__ out) {
-  const BatchInstance& I = insts[blockIdx.x];
+__global__ void k6_expect_finish(const double* __restrict__ partial, double* __restrict__ out) {
   if (threadIdx.x != 0) return;
-  const int cb = I.n < kChunkBits ? I.n : kChunkBits;
-  const uint64_t nchunks = 1ull << (I.n - cb);
   double s = 0;
-  for (uint64_t c = 0; c < nchunks; ++c) s += partial[size_t(blockIdx.x) * max_chunks + c];
+  for (int b = 0; b < kExpectBlocks; ++b) s += partial[size_t(blockIdx.x) * kExpectBlocks + b];
   out[blockIdx.x] = s;
 }
 
 }  // namespace
 
+int batch_max_ctas_per_sm() {
+  int n = 0;
+  if (cudaFuncSetAttribute(k6_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(kBatchSmem)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k6_batch, kBatchThreads, kBatchSmem) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  return n < 1 ? 1 : n;
+}
+
 int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
                  int ngroups, uint64_t total_items, uint32_t* d_counters,
                  unsigned long long* d_head, int* d_err, int grid, cudaStream_t s) {
-  k6_batch<<<grid, kBatchThreads, 0, s>>>(d_inst, d_par, d_items, ngroups, total_items,
-                                          d_counters, d_head, d_err);
+  HS_CUDA(cudaFuncSetAttribute(k6_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(kBatchSmem)));
+  k6_batch<<<grid, kBatchThreads, kBatchSmem, s>>>(d_inst, d_par, d_items, ngroups, total_items,
+                                                   d_counters, d_head, d_err);
   HS_CUDA(cudaGetLastError());
   return HS_OK;
 }
@@ -281,11 +338,12 @@ int launch_batch_init(const BatchInstance* d_inst, int ninst, cudaStream_t s) {
   return HS_OK;
 }
 
+// d_partial: ninst x kExpectBlocks doubles
 int launch_batch_expect(const BatchInstance* d_inst, int ninst, int max_n, double* d_partial,
                         double* d_out, cudaStream_t s) {
-  const int max_chunks = 1 << (max_n > kChunkBits ? max_n - kChunkBits : 0);
-  k6_expect<<<dim3(max_chunks, ninst), 256, 0, s>>>(d_inst, d_partial, max_chunks);
-  k6_expect_finish<<<ninst, 32, 0, s>>>(d_inst, d_partial, max_chunks, d_out);
+  (void)max_n;
+  k6_expect<<<dim3(kExpectBlocks, ninst), 256, 0, s>>>(d_inst, d_partial);
+  k6_expect_finish<<<ninst, 32, 0, s>>>(d_partial, d_out);
   HS_CUDA(cudaGetLastError());
   return HS_OK;
 }
