@@ -90,6 +90,7 @@ SIGNATURES = {
     "hs_part_features": [_i, _i, _vp, _i, _vp, _vp, _i, _vp],
     "hs_order_segments": [_i, _i, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _vp],
     "hs_parts_run_timed": [_vp, _vp, _vp, _i, _vp, _vp],
+    "hs_project": [_vp, _vp, _vp, _i, _i, ctypes.POINTER(_vp), _dp, _vp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
@@ -179,6 +180,22 @@ class State:
 
     def set_basis(self, x: int, stream=None):
         check(lib().hs_state_set_basis(self.h, x, stream))
+
+    @classmethod
+    def _wrap(cls, handle, n: int, dtype: int) -> "State":
+        st = cls.__new__(cls)
+        st.h, st.n, st.dtype = handle, n, dtype
+        return st
+
+    def project(self, qubits, values=None, norm_mode: int = 0):
+        """hs_project: (new state over the remaining qubits, probability)."""
+        q = np.ascontiguousarray(qubits, dtype=np.int32)
+        v = None if values is None else np.ascontiguousarray(values, dtype=np.int32)
+        h = _vp()
+        p = ctypes.c_double()
+        check(lib().hs_project(self.h, _ptr(q), _ptr(v), len(q), norm_mode, ctypes.byref(h),
+                               ctypes.byref(p), None))
+        return State._wrap(h, self.n - len(q), self.dtype), p.value
 
     def qubit_to_slot(self) -> np.ndarray:
         out = np.zeros(self.n, dtype=np.int32)

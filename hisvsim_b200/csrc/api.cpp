@@ -2,6 +2,7 @@
 // points, redistribution and reductions.  Every function returns a status and
 // never aborts; messages are kept per calling thread.
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -452,6 +453,47 @@ int hs_gather_qubits(hs_state* st, const int32_t* proc_qubits, int num, void* st
   for (int j = 0; j < st->n; ++j) pi[order[j]] = j;
   TimedRegion tr(S(stream));
   return permute_positions(st, pi, S(stream));
+}
+
+int hs_project(hs_state* st, const int32_t* qubits, const int32_t* values, int count,
+               int norm_mode, hs_state** out, double* prob_out, void* stream) {
+  HS_TRY(check_state(st));
+  if (!out) return set_error(HS_E_INVALID, "null output pointer");
+  *out = nullptr;
+  if (count < 1 || count >= st->n || !qubits)
+    return set_error(HS_E_INVALID, "project 1..%d of %d qubits", st->n - 1, st->n);
+  if (norm_mode < 0 || norm_mode > 2) return set_error(HS_E_INVALID, "norm mode 0, 1 or 2");
+  std::vector<char> used(st->n, 0);
+  uint64_t offset = 0;
+  for (int i = 0; i < count; ++i) {
+    const int q = qubits[i], v = values ? values[i] : 0;
+    if (q < 0 || q >= st->n || used[q]) return set_error(HS_E_INVALID, "bad or repeated qubit");
+    if (v != 0 && v != 1) return set_error(HS_E_INVALID, "values must be 0 or 1");
+    used[q] = 1;
+    offset |= uint64_t(v) << st->q2s[q];
+  }
+  std::vector<int> slots;
+  for (int q = 0; q < st->n; ++q)
+    if (!used[q]) slots.push_back(st->q2s[q]);
+  hs_state* ns = nullptr;
+  HS_TRY(hs_state_create(st->n - count, st->dtype, &ns));
+  const cudaStream_t s = S(stream);
+  double p = 0;
+  int rc = project_kernel(st->amp, ns->amp, st->dtype, ns->n, slots.data(), offset, s);
+  if (rc == HS_OK) rc = reduce_norm2(ns->amp, ns->dtype, ns->n, &p, s);
+  // the reference divides by p (state_vector.hpp:867-882) and skips p <= 1e-12
+  if (rc == HS_OK && norm_mode != 2 && p > 1e-12)
+    rc = scale_kernel(ns->amp, ns->dtype, ns->n, norm_mode == 0 ? 1.0 / std::sqrt(p) : 1.0 / p,
+                      s);
+  if (rc == HS_OK && cudaStreamSynchronize(s) != cudaSuccess)
+    rc = set_error(HS_E_CUDA, "project: synchronize");
+  if (rc != HS_OK) {
+    hs_state_destroy(ns);
+    return rc;
+  }
+  if (prob_out) *prob_out = p;
+  *out = ns;
+  return HS_OK;
 }
 
 int hs_norm2(hs_state* st, double* out) {

@@ -236,6 +236,10 @@ int reduce_zz(const void* amp, int dtype, int n, const int32_t* slot_pairs, int 
 int reduce_chunks(const void* amp, int dtype, int n, int chunk_bits, double* host_out,
                   cudaStream_t s);
 int set_basis_kernel(void* amp, int dtype, int n, uint64_t index, cudaStream_t s);
+// out[j] = in[offset | deposit(j, old_slots)] for j < 2^out_bits
+int project_kernel(const void* in, void* out, int dtype, int out_bits, const int* old_slots,
+                   uint64_t offset, cudaStream_t s);
+int scale_kernel(void* amp, int dtype, int n, double f, cudaStream_t s);
 int convert_kernel(const void* src, int sdtype, void* dst, int ddtype, uint64_t count,
                    cudaStream_t s);
 

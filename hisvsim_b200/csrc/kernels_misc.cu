@@ -383,6 +383,63 @@ int reduce_zz(const void* amp, int dtype, int n, const int32_t* slot_pairs, int 
   return HS_OK;
 }
 
+namespace {
+struct ProjectMap {
+  int32_t nbits;
+  uint8_t slot[40];  // old slot of each bit of the projected index
+};
+
+template <typename T>
+__global__ void k_project(const T* __restrict__ in, T* __restrict__ out, uint64_t count,
+                          ProjectMap map, uint64_t offset) {
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < count;
+       j += uint64_t(gridDim.x) * blockDim.x) {
+    uint64_t src = offset;
+    for (int b = 0; b < map.nbits; ++b) src |= ((j >> b) & 1ull) << map.slot[b];
+    out[j] = in[src];
+  }
+}
+
+template <typename T>
+__global__ void k_scale(T* __restrict__ a, uint64_t count, double f) {
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < count;
+       j += uint64_t(gridDim.x) * blockDim.x) {
+    T v = a[j];
+    v.x = decltype(v.x)(v.x * f);
+    v.y = decltype(v.y)(v.y * f);
+    a[j] = v;
+  }
+}
+}  // namespace
+
+int project_kernel(const void* in, void* out, int dtype, int out_bits, const int* old_slots,
+                   uint64_t offset, cudaStream_t s) {
+  ProjectMap map{};
+  map.nbits = out_bits;
+  for (int b = 0; b < out_bits; ++b) map.slot[b] = uint8_t(old_slots[b]);
+  const uint64_t count = 1ull << out_bits;
+  const int g = grid_for(count, 256);
+  if (dtype == HS_DTYPE_C128)
+    k_project<double2><<<g, 256, 0, s>>>(static_cast<const double2*>(in),
+                                         static_cast<double2*>(out), count, map, offset);
+  else
+    k_project<float2><<<g, 256, 0, s>>>(static_cast<const float2*>(in),
+                                        static_cast<float2*>(out), count, map, offset);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
+int scale_kernel(void* amp, int dtype, int n, double f, cudaStream_t s) {
+  const uint64_t count = 1ull << n;
+  const int g = grid_for(count, 256);
+  if (dtype == HS_DTYPE_C128)
+    k_scale<double2><<<g, 256, 0, s>>>(static_cast<double2*>(amp), count, f);
+  else
+    k_scale<float2><<<g, 256, 0, s>>>(static_cast<float2*>(amp), count, f);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
 int set_basis_kernel(void* amp, int dtype, int n, uint64_t index, cudaStream_t s) {
   const uint64_t size = 1ull << n;
   if (dtype == HS_DTYPE_C128)

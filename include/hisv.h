@@ -248,6 +248,15 @@ int hs_expect_zz(hs_state* st, const int32_t* pairs, int num_pairs, double* out)
 int hs_measure(hs_state* st, const int32_t* qubits, int num_qubits,
                uint32_t num_samples, uint64_t seed, int32_t* out);
 
+/* Projection (StateVector::project, state_vector.hpp:829-894): the part of
+ * the state with qubits[i] = values[i] (values NULL: all 0) as a NEW state
+ * over the remaining qubits, renumbered 0.. in increasing order.  norm_mode
+ * 0 divides by sqrt(p), 1 divides by p as the reference does, 2 leaves it
+ * unnormalised (the reference's renormalize=false); p <= 1e-12 is left as is.
+ * *prob_out = p = the squared norm of the projected part (may be NULL). */
+int hs_project(hs_state* st, const int32_t* qubits, const int32_t* values, int count,
+               int norm_mode, hs_state** out, double* prob_out, void* stream);
+
 /* ---- batching form (no counterpart in the reference) -----------------------
  * Many QAOA MaxCut circuits of different qubit counts (parameter sweeps), all
  * advanced by one persistent launch (K6) replayed as a captured CUDA graph:

@@ -108,3 +108,41 @@ def test_measure_distribution():
     counts = np.bincount(idx, minlength=1 << n) / len(idx)
     assert np.abs(counts - p).max() < 0.02
     assert np.array_equal(st.measure([0, 3], 50, 99), st.measure([0, 3], 50, 99))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("dtype", [abi.C128, abi.C64])
+def test_project_matches_numpy(mode, dtype):
+    """hs_project (state_vector.hpp:829-894) against a numpy restatement, on a
+    state whose slots are permuted (qubit q not at slot q)."""
+    n = 9
+    gates = circuits.random_layered(n, 6, 31)
+    st = abi.State(n, dtype)
+    st.set_basis(0)
+    for g in gates:
+        st.apply(g)
+    st.permute_bits([(0, 7), (2, 5)])
+    full = st.amplitudes().astype(np.complex128)
+    st.permute_bits([(0, 7), (2, 5)])
+    qubits, values = [6, 1, 3], [1, 0, 1]
+    sub, p = st.project(qubits, values, mode)
+    idx = np.arange(1 << n)
+    keep = np.ones(1 << n, dtype=bool)
+    for q, v in zip(qubits, values):
+        keep &= ((idx >> q) & 1) == v
+    want = full[keep]  # remaining qubits in increasing order = ascending index
+    wp = float(np.sum(np.abs(want) ** 2))
+    tol = 1e-12 if dtype == abi.C128 else 1e-5
+    assert p == pytest.approx(wp, rel=tol, abs=tol)
+    want = want / (np.sqrt(wp) if mode == 0 else wp if mode == 1 else 1.0)
+    assert sub.n == n - 3
+    assert np.abs(sub.amplitudes() - want).max() <= tol * max(1.0, np.abs(want).max())
+    if mode == 0:
+        assert sub.norm2() == pytest.approx(1.0, abs=tol)
+
+
+def test_project_rejects_bad_arguments():
+    st = abi.State(4)
+    for q, v in ([[0, 0], [0, 1]], [[5], [0]], [[1], [2]], [[0, 1, 2, 3], None]):
+        with pytest.raises(abi.HisvError):
+            st.project(q, v)
