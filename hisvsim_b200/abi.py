@@ -91,6 +91,7 @@ SIGNATURES = {
     "hs_order_segments": [_i, _i, _vp, _i, _vp, _i, _i, _i, _vp, _vp, _vp, _vp],
     "hs_parts_run_timed": [_vp, _vp, _vp, _i, _vp, _vp],
     "hs_project": [_vp, _vp, _vp, _i, _i, ctypes.POINTER(_vp), _dp, _vp],
+    "hs_fp64_peak": [_dp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
@@ -531,6 +532,13 @@ class QaoaBatch:
             self.close()
         except Exception:
             pass
+
+
+def fp64_peak_tflops() -> float:
+    """Measured FP64 FMA throughput of the current device (TFLOP/s)."""
+    out = ctypes.c_double()
+    check(lib().hs_fp64_peak(ctypes.byref(out)))
+    return out.value
 
 
 def set_tile_qubits(m: int) -> int:

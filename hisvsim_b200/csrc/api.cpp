@@ -496,6 +496,11 @@ int hs_project(hs_state* st, const int32_t* qubits, const int32_t* values, int c
   return HS_OK;
 }
 
+int hs_fp64_peak(double* tflops) {
+  if (!tflops) return set_error(HS_E_INVALID, "null output");
+  return fp64_probe(tflops);
+}
+
 int hs_norm2(hs_state* st, double* out) {
   HS_TRY(check_state(st));
   return reduce_norm2(st->amp, st->dtype, st->n, out, nullptr);

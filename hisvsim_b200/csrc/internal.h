@@ -240,6 +240,7 @@ int set_basis_kernel(void* amp, int dtype, int n, uint64_t index, cudaStream_t s
 int project_kernel(const void* in, void* out, int dtype, int out_bits, const int* old_slots,
                    uint64_t offset, cudaStream_t s);
 int scale_kernel(void* amp, int dtype, int n, double f, cudaStream_t s);
+int fp64_probe(double* tflops);
 int convert_kernel(const void* src, int sdtype, void* dst, int ddtype, uint64_t count,
                    cudaStream_t s);
 

@@ -440,6 +440,52 @@ int scale_kernel(void* amp, int dtype, int n, double f, cudaStream_t s) {
   return HS_OK;
 }
 
+namespace {
+// FP64 FMA throughput probe: 8 independent chains per thread
+__global__ void k_fma_probe(double* out, double a, double b, int iters) {
+  double r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = double(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r[k] = fma(r[k], a, b);
+  }
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += r[k];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live; never true in practice
+}
+}  // namespace
+
+int fp64_probe(double* tflops) {
+  int dev = 0, sms = 148;
+  HS_CUDA(cudaGetDevice(&dev));
+  HS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  double* d = nullptr;
+  HS_CUDA(cudaMalloc(&d, sizeof(double)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(e0);
+    k_fma_probe<<<blocks, threads>>>(d, 0.999999, 1e-7, iters);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  const cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_error(HS_E_CUDA, "fp64 probe: %s", cudaGetErrorString(e));
+  *tflops = 2.0 * 8.0 * double(iters) * blocks * threads / (double(best) * 1e-3) / 1e12;
+  return HS_OK;
+}
+
 int set_basis_kernel(void* amp, int dtype, int n, uint64_t index, cudaStream_t s) {
   const uint64_t size = 1ull << n;
   if (dtype == HS_DTYPE_C128)

@@ -257,6 +257,10 @@ int hs_measure(hs_state* st, const int32_t* qubits, int num_qubits,
 int hs_project(hs_state* st, const int32_t* qubits, const int32_t* values, int count,
                int norm_mode, hs_state** out, double* prob_out, void* stream);
 
+/* Measured FP64 FMA throughput of this device (TFLOP/s, 2 flops per FMA):
+ * the compute roofline of the complex128 part kernel. */
+int hs_fp64_peak(double* tflops);
+
 /* ---- batching form (no counterpart in the reference) -----------------------
  * Many QAOA MaxCut circuits of different qubit counts (parameter sweeps), all
  * advanced by one persistent launch (K6) replayed as a captured CUDA graph:
