@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=512)
     ap.add_argument("--batch-check", type=int, default=512,
                     help="instances whose <H_C> is checked against complex128 plain runs")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned form")
+    ap.add_argument("--learned-qubits", type=int, default=34)
+    ap.add_argument("--learned-parts", type=int, default=20000, help="part timings harvested")
     return ap.parse_args()
 
 
@@ -266,6 +269,59 @@ def batch_form(args, abi, peak_gbs, pg, device):
             "dtype": "c64 states, fp64 <H_C>", "clocks": clk.summary()}
 
 
+def learned_form(args, abi, pg, device):
+    """Learned form: harvest part timings (complex64, random circuits of
+    24-32 qubits), train the cost model with the library's K7 kernels, let it
+    propose part sizes and cut points for a complex64 random circuit
+    (``--learned-qubits`` qubits x 40 layers, U3 + CZ), and time that against
+    the acyclic partitioner (the fallback) at its default and best part size."""
+    import numpy as np
+
+    from hisvsim_b200 import circuits, learned, partition
+
+    weights = {24: 4000, 25: 3500, 26: 3000, 27: 2500, 28: 2500, 29: 1800, 30: 1400, 31: 800,
+               32: 500}
+    total_w = sum(weights.values())
+    counts = {n: max(50, int(w * args.learned_parts / total_w)) for n, w in weights.items()}
+    t0 = time.perf_counter()
+    X, y, ns, _ = learned.harvest(counts, seed=args.seed)
+    t_h = time.perf_counter() - t0
+    rng = np.random.default_rng(args.seed)
+    perm = rng.permutation(len(y))
+    ntr = int(0.9 * len(y))
+    model = learned.CostModel(seed=args.seed)
+    t0 = time.perf_counter()
+    losses = model.fit(X[perm[:ntr]], y[perm[:ntr]], epochs=150, batch=256, lr=2e-3)
+    t_t = time.perf_counter() - t0
+    te = perm[ntr:]
+    rel = float(np.mean(np.abs(np.exp(model.predict_target(X[te]) - y[te]) - 1)))
+    n = args.learned_qubits
+    gates = circuits.random_u3_cz(n, 40, args.seed + 34)
+    t0 = time.perf_counter()
+    prop = learned.propose(gates, n, model)
+    t_p = time.perf_counter() - t0
+    st = abi.State(n, abi.C64)
+    ks = [9] + [k for k in (7, 8, 10) if f"acyclic k={k}" in prop["candidates"]]
+    res = {}
+    with ClockSampler(device) as clk:
+        t_learned = learned.measure(st, gates, prop["parts"], reps=1, warmup=0)
+        for k in ks:
+            res[k] = learned.measure(st, gates, partition.partition_acyclic(gates, k), reps=1,
+                                     warmup=0)
+    st.close()
+    model.close()
+    best_k = min(res, key=res.get)
+    return {"harvest_parts": int(len(y)), "harvest_qubits": "24..32", "harvest_s": t_h,
+            "train_s": t_t, "final_train_mse": float(losses[-1]), "holdout_mean_rel_err": rel,
+            "eval": f"random U3+CZ circuit {n} qubits x 40 layers, complex64",
+            "proposal": prop["method"], "proposal_parts": len(prop["parts"]),
+            "propose_s": t_p, "learned_s": t_learned,
+            "acyclic_s": {str(k): v for k, v in res.items()},
+            "gain_vs_acyclic_k9": res[9] / t_learned,
+            "gain_vs_best_acyclic": res[best_k] / t_learned, "best_acyclic_k": best_k,
+            "clocks": clk.summary()}
+
+
 def timed_steps(abi, step, warmup, steps, pg, device):
     """W untimed steps, then K steps between events on the library stream."""
     for _ in range(warmup):
@@ -410,6 +466,10 @@ def main():
     if not args.no_batch:
         batch = batch_form(args, abi, peak_gbs, pg, local)
 
+    learned_res = None
+    if not args.no_learned and rank == 0:
+        learned_res = learned_form(args, abi, pg, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -439,6 +499,7 @@ def main():
                          "avg_launch_ms": k1_avg_ms},
             "fused": fused,
             "batch": batch,
+            "learned": learned_res,
             "gpu_launches": int(c["passes"] + args.steps),
             "launch_param_bytes_per_step": pbytes / args.steps,
             "clocks": clk,

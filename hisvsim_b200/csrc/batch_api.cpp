@@ -15,7 +15,7 @@ struct hs_batch {
   std::vector<int> n;
   std::vector<std::vector<std::pair<int, int>>> edges;
   std::vector<double> gammas, betas;
-  int tile_cap = 12, ctas_per_sm = 3, chunk = 8;
+  int tile_cap = kBatchMaxTileBits, ctas_per_sm = 6, chunk = 8;
   int cap_of_n[kBatchMaxQubits + 1] = {};  // per qubit count; 0 = tile_cap
   void* pool = nullptr;
   std::vector<uint64_t> offset;  // amplitude offset of each instance in the pool
@@ -356,8 +356,8 @@ int hs_batch_set_chunk(hs_batch* b, int tiles_per_item) {
 
 int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm) {
   if (!b) return set_error(HS_E_INVALID, "null batch");
-  if (tile_cap < 6 || tile_cap > 12 || ctas_per_sm < 1 || ctas_per_sm > 8)
-    return set_error(HS_E_INVALID, "tile cap 6..12, 1..8 CTAs per SM");
+  if (tile_cap < 6 || tile_cap > kBatchMaxTileBits || ctas_per_sm < 1 || ctas_per_sm > 16)
+    return set_error(HS_E_INVALID, "tile cap 6..%d, 1..16 CTAs per SM", kBatchMaxTileBits);
   const int old_cap = b->tile_cap, old_ctas = b->ctas_per_sm;
   b->tile_cap = tile_cap;
   b->ctas_per_sm = ctas_per_sm;
@@ -393,8 +393,8 @@ int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* be
   double best = 1e300;
   const int maxc = batch_max_ctas_per_sm();
   int bc = b->tile_cap, bt = b->ctas_per_sm, bk = b->chunk;
-  for (int cap : {10, 11, 12})
-    for (int ctas : {std::max(1, maxc - 1), maxc})
+  for (int cap : {9, 10, 11})
+    for (int ctas : {std::max(1, maxc - 2), maxc})
       for (int chunk : {4, 16}) {
         b->chunk = chunk;
         if (hs_batch_configure(b, cap, ctas) != HS_OK) continue;
@@ -416,10 +416,10 @@ int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* be
   ns.erase(std::unique(ns.begin(), ns.end()), ns.end());
   std::reverse(ns.begin(), ns.end());
   for (int n : ns) {
-    if (n <= 10) continue;  // one pass whatever the cap
+    if (n <= 9) continue;  // one pass whatever the cap
     const int keep = b->cap_of_n[n];
     int chosen = keep;
-    for (int cap : {10, 11, 12}) {
+    for (int cap : {9, 10, 11}) {
       if (cap == (keep ? keep : bc)) continue;
       b->cap_of_n[n] = cap;
       if (build_plan(b) != HS_OK) continue;

@@ -177,8 +177,9 @@ int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, u
 constexpr int kBatchMaxQubits = 30;
 constexpr int kBatchMaxEdges = 64;
 constexpr int kBatchMaxRounds = 8;
-constexpr int kBatchMaxPasses = 4;   // passes per round (tile <= 12 bits, 9 new qubits each)
-constexpr int kBatchThreads = 256;
+constexpr int kBatchMaxPasses = 4;   // passes per round (tile <= 11 bits, 8 new qubits each)
+constexpr int kBatchThreads = 128;   // 16 amplitudes per thread: tiles of up to 2^11
+constexpr int kBatchMaxTileBits = 11;
 
 // one pass of a QAOA round over an instance: the tile bits, which of them get
 // the mixer RX, in register groups of 4 (tile-bit positions)

@@ -20,7 +20,7 @@
 namespace hisv {
 namespace {
 
-constexpr int kTileMax = 4096;
+constexpr int kTileMax = 1 << kBatchMaxTileBits;
 constexpr uint32_t kDepLimit = 1u << 24;  // polls (with ~0.1 us sleeps) before giving up
 
 __device__ __forceinline__ uint64_t bdep(uint64_t x, const Runs& r) {
@@ -47,6 +47,7 @@ struct Shared {
   float2 phase[kBatchMaxEdges + 1];
   uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
   uint8_t cut[kTileMax];
+  uint64_t gk[kTileMax / 2 / kBatchThreads];  // global offset of chunk k*threads
   int w[16];
   int c;
   int group;
@@ -78,7 +79,7 @@ __device__ __forceinline__ void cross_weights(Shared& S, int nedges, int m, uint
   if (lane == 0) S.c = c;
 }
 
-__global__ void __launch_bounds__(kBatchThreads, 3)
+__global__ void __launch_bounds__(kBatchThreads, 6)
     k6_batch(const BatchInstance* __restrict__ insts, const BatchParams* __restrict__ pars,
              const BatchItem* __restrict__ groups, int ngroups, uint64_t total,
              uint32_t* __restrict__ counters, unsigned long long* __restrict__ head,
@@ -140,20 +141,31 @@ __global__ void __launch_bounds__(kBatchThreads, 3)
     }
     const float2 rx = pars[G.inst].rx[round][0];  // (cos beta, sin beta)
     const bool active = t < (T >> 4);
-    // thread bits of each register group: the tile bits not held in registers
-    uint32_t thr[3] = {0, 0, 0};
+    // 16-byte chunk c = t + k * threads covers tile indices 2c, 2c + 1; the
+    // bits of t and of k * threads are disjoint, so its global offset is
+    // bdep(2t) + bdep(2k * threads)
+    const int nck = (T / 2 + kBatchThreads - 1) / kBatchThreads;
+    if (t < nck) S.gk[t] = bdep(2ull * uint64_t(t) * kBatchThreads, P.tile);
+    const uint64_t gt = bdep(2ull * t, P.tile);
+    // thread bits of each register group: the tile bits not held in registers;
+    // bswz is linear over GF(2), so a register element's slot is
+    // bswz(thread part) ^ (XOR of bswz(register bit))
+    uint32_t sbase[3] = {0, 0, 0}, thr0 = 0;
     for (int g = 0; g < ngr; ++g) {
-      uint32_t rmask = 0;
+      uint32_t rmask = 0, thr = 0;
       for (int j = 0; j < 4; ++j) rmask |= 1u << P.group_bits[g][j];
       int src = 0;
       for (int b = 0; b < m; ++b)
-        if (!((rmask >> b) & 1u)) thr[g] |= uint32_t((t >> src++) & 1) << b;
+        if (!((rmask >> b) & 1u)) thr |= uint32_t((t >> src++) & 1) << b;
+      sbase[g] = bswz(thr);
+      if (g == 0) thr0 = thr;
     }
+    __syncthreads();  // S.gk
     // prologue: first tile into buffer 0
     {
-      const uint64_t gbase = bdep(t_begin, P.outer);
-      for (int c = t; c < T / 2; c += kBatchThreads)
-        cp16(tiles_s + bswz(2u * uint32_t(c)) * 8u, amp + gbase + bdep(2ull * c, P.tile));
+      const uint64_t gb = bdep(t_begin, P.outer) + gt;
+      for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads)
+        cp16(tiles_s + bswz(2u * uint32_t(c)) * 8u, amp + gb + S.gk[k]);
       cp_commit();
     }
     for (uint32_t ti = t_begin; ti < t_end; ++ti) {
@@ -162,10 +174,10 @@ __global__ void __launch_bounds__(kBatchThreads, 3)
       const uint64_t gbase = bdep(ti, P.outer);
       __syncthreads();  // the other buffer's previous tile is fully stored
       if (ti + 1 < t_end) {
-        const uint64_t nbase = bdep(ti + 1, P.outer);
+        const uint64_t nb = bdep(ti + 1, P.outer) + gt;
         const uint32_t ns = tiles_s + uint32_t((buf ^ 1) * kTileMax * 8);
-        for (int c = t; c < T / 2; c += kBatchThreads)
-          cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nbase + bdep(2ull * c, P.tile));
+        for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads)
+          cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nb + S.gk[k]);
         cp_commit();
         cp_wait<1>();
       } else {
@@ -175,29 +187,33 @@ __global__ void __launch_bounds__(kBatchThreads, 3)
       __syncthreads();
       for (int g = 0; g < ngr; ++g) {
         if (active) {
-          uint32_t rb[4];
+          uint32_t so[4];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) rb[j] = 1u << P.group_bits[g][j];
+          for (int j = 0; j < 4; ++j) so[j] = bswz(1u << P.group_bits[g][j]);
           float2 v[16];
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
-            uint32_t idx = thr[g];
+            uint32_t a = sbase[g];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-              if ((e >> j) & 1) idx |= rb[j];
-            v[e] = tile[bswz(idx)];
+              if ((e >> j) & 1) a ^= so[j];
+            v[e] = tile[a];
           }
           if (g == 0 && phase) {
             // cut = cut_low[i] + C + sum_q w_q i_q (tile bit q is qubit q)
             int dthr = S.c;
             for (int b = 0; b < m; ++b)
-              if ((thr[0] >> b) & 1u) dthr += S.w[b];
+              if ((thr0 >> b) & 1u) dthr += S.w[b];
             int wr[4];
+            uint32_t rb[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) wr[j] = S.w[P.group_bits[0][j]];
+            for (int j = 0; j < 4; ++j) {
+              wr[j] = S.w[P.group_bits[0][j]];
+              rb[j] = 1u << P.group_bits[0][j];
+            }
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
-              uint32_t idx = thr[0];
+              uint32_t idx = thr0;
               int cc = dthr;
 #pragma unroll
               for (int j = 0; j < 4; ++j)
@@ -225,18 +241,21 @@ __global__ void __launch_bounds__(kBatchThreads, 3)
           }
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
-            uint32_t idx = thr[g];
+            uint32_t a = sbase[g];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
-              if ((e >> j) & 1) idx |= rb[j];
-            tile[bswz(idx)] = v[e];
+              if ((e >> j) & 1) a ^= so[j];
+            tile[a] = v[e];
           }
         }
         __syncthreads();
       }
-      for (int c = t; c < T / 2; c += kBatchThreads) {
-        const uint4 d = *reinterpret_cast<const uint4*>(&tile[bswz(2u * uint32_t(c))]);
-        *reinterpret_cast<uint4*>(amp + gbase + bdep(2ull * c, P.tile)) = d;
+      {
+        const uint64_t gb = gbase + gt;
+        for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads) {
+          const uint4 d = *reinterpret_cast<const uint4*>(&tile[bswz(2u * uint32_t(c))]);
+          *reinterpret_cast<uint4*>(amp + gb + S.gk[k]) = d;
+        }
       }
     }
     __threadfence();

@@ -275,7 +275,7 @@ int hs_batch_create_qaoa(int num_instances, const int32_t* num_qubits,
                          const double* gammas, const double* betas, hs_batch** out);
 /* New angles for the next run (the captured graph is reused). */
 int hs_batch_set_params(hs_batch* b, const double* gammas, const double* betas);
-/* Tile cap (6..12 qubits per pass) and persistent CTAs per SM (clamped to
+/* Tile cap (6..11 qubits per pass) and persistent CTAs per SM (clamped to
  * what fits on an SM). */
 int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm);
 /* Tiles per work item (a dequeued chunk of one step of one instance). */
