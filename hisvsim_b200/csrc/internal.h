@@ -124,7 +124,9 @@ static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
               int tile_bits_hint, int dtype, std::vector<PartProgram>* programs);
 int current_tile_hint();  // hs_set_tile_qubits' value
-inline int max_tile_bits(int dtype) { (void)dtype; return 12; }
+// complex128 tiles stop at 2^11 so that three CTAs (two 32 KiB buffers each,
+// <= 168 registers per thread) share an SM; complex64 tiles go to 2^12
+inline int max_tile_bits(int dtype) { return dtype == HS_DTYPE_C64 ? 12 : 11; }
 
 // ---- K2 bit-swap program ----------------------------------------------------
 struct PermProgram {

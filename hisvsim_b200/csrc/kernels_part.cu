@@ -326,15 +326,23 @@ __device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32
   (void)M::SH;
 }
 
-// tiles are at most 2^12 amplitudes (two buffers of 64 KiB for complex128):
-// 2^(12-R) = 256 threads
+// complex64 tiles are at most 2^12 amplitudes: 2^(12-R) = 256 threads, one
+// CTA per SM bound; complex128 tiles at most 2^11: 128 threads, and the
+// register bound leaves room for three CTAs per SM (FP64-heavy passes need
+// the extra warps to hide latency)
 template <typename V>
 struct K1Threads {
   static constexpr int value = 256;
+  static constexpr int min_blocks = 1;
+};
+template <>
+struct K1Threads<double2> {
+  static constexpr int value = 128;
+  static constexpr int min_blocks = 3;
 };
 
 template <int R, bool FULL, typename V>
-__global__ void __launch_bounds__(K1Threads<V>::value, 1)
+__global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
     k1_part(V* __restrict__ sv, const __grid_constant__ PartProgram P) {
   using M = SmemMap<V>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -381,17 +389,15 @@ __global__ void __launch_bounds__(K1Threads<V>::value, 1)
         lo[j] = (b & ((1u << M::SH) - 1u)) * uint32_t(sizeof(V));
       }
       const uint32_t sthr = M::off(thr);
-      uint32_t addr[E];
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
+      auto addr = [&](int e) -> uint32_t {
         uint32_t a = sthr;
 #pragma unroll
         for (int j = 0; j < R; ++j)
           if ((e >> j) & 1) a = (a ^ sx[j]) + lo[j];
-        addr[e] = a;
-      }
+        return a;
+      };
 #pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(A + addr[e]);
+      for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(A + addr(e));
       // op descriptors and coefficients are read from the (warp-uniform)
       // parameter space, so every dispatch below is a uniform branch
       int o = G.first_op;
@@ -406,7 +412,7 @@ __global__ void __launch_bounds__(K1Threads<V>::value, 1)
         op_inplace<R, FULL>(v, op, P.coef + op.coef, thr, gbase);
       }
 #pragma unroll
-      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr[e]) = v[e];
+      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr(e)) = v[e];
       goto group_done;
     in_w:
       while (o < o_end) {
@@ -418,7 +424,7 @@ __global__ void __launch_bounds__(K1Threads<V>::value, 1)
         op_inplace<R, FULL>(w, op, P.coef + op.coef, thr, gbase);
       }
 #pragma unroll
-      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr[e]) = w[e];
+      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr(e)) = w[e];
     group_done:
       __syncthreads();  // the group's writes precede the next group's reads
     }
