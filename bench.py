@@ -425,6 +425,15 @@ def main():
         traffic = tr.get("bytes_per_launch_scaled")
     except Exception:
         pass
+    # FP64 work of the plain pass: 8 FMA per amplitude for every dense
+    # one-qubit gate (U3), none for the CZ sign flips
+    dense = sum(1 for g in gates if g.name == "U3")
+    fma_step = dense * 8.0 * float(1 << n)
+    fp64_peak = abi.fp64_peak_tflops()
+    k1_total_s = c["apply_us"] / 1e6 / args.steps
+    fp64 = {"fma_per_step": fma_step, "achieved_tflops": 2 * fma_step / k1_total_s / 1e12,
+            "peak_tflops": fp64_peak, "source": "hs_fp64_peak (measured FP64 FMA probe)",
+            "frac": 2 * fma_step / k1_total_s / 1e12 / fp64_peak}
     st.close()
     del st
 
@@ -496,7 +505,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": k1_gbs, "peak": peak_gbs, "unit": "GB/s",
                          "frac": k1_gbs / peak_gbs, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "k1_part", "algorithmic_bytes_per_launch": bytes_per_pass,
-                         "avg_launch_ms": k1_avg_ms},
+                         "avg_launch_ms": k1_avg_ms, "fp64": fp64},
             "fused": fused,
             "batch": batch,
             "learned": learned_res,

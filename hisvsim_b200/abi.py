@@ -92,6 +92,8 @@ SIGNATURES = {
     "hs_parts_run_timed": [_vp, _vp, _vp, _i, _vp, _vp],
     "hs_project": [_vp, _vp, _vp, _i, _i, ctypes.POINTER(_vp), _dp, _vp],
     "hs_fp64_peak": [_dp],
+    "hs_set_fused_shape": [_i, _i],
+    "hs_fused_apply": [_vp, _vp, _vp, _i, _vp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
     "hs_norm2": [_vp, _dp],
@@ -251,6 +253,12 @@ class State:
         offsets = np.ascontiguousarray(offsets, dtype=np.int32)
         check(lib().hs_fused_parts_run(self.h, _ptr(records), _ptr(offsets), len(offsets) - 1,
                                        precision, stream))
+
+    def fused_apply(self, u, qubits, precision: int = 0, stream=None):
+        """hs_fused_apply: a 64x64 unitary on six qubits (bit j of the index = qubits[j])."""
+        u = np.ascontiguousarray(u, dtype=np.complex128).reshape(64, 64)
+        q = np.ascontiguousarray(qubits, dtype=np.int32)
+        check(lib().hs_fused_apply(self.h, _ptr(u), _ptr(q), precision, stream))
 
     def compare(self, other: "State") -> dict:
         """<self|other>, max |self - other|, <other|other> and the fidelity."""
@@ -532,6 +540,13 @@ class QaoaBatch:
             self.close()
         except Exception:
             pass
+
+
+def set_fused_shape(max_ops_per_pass: int, tile_bits: int) -> int:
+    r = lib().hs_set_fused_shape(max_ops_per_pass, tile_bits)
+    if r < 0:
+        check(r)
+    return r
 
 
 def fp64_peak_tflops() -> float:

@@ -92,6 +92,11 @@ int plan_passes(int n, int cap, BatchInstance* I) {
         tl.push_back(q);
         tg.push_back(q);
       }
+      // widen the tile with the next-lowest qubits (no gate on them in this
+      // pass): fewer, larger tiles and longer contiguous runs
+      for (int q = 3; q < n && int(tl.size()) < cap; ++q)
+        if (std::find(tl.begin(), tl.end(), q) == tl.end()) tl.push_back(q);
+      std::sort(tl.begin(), tl.end());
       tiles.push_back(tl);
       targets.push_back(tg);
       covered += nw;

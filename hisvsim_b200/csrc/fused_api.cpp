@@ -6,6 +6,8 @@
 #include <cstring>
 #include <vector>
 
+#include <atomic>
+
 #include "internal.h"
 
 namespace hisv {
@@ -113,15 +115,19 @@ void runs_of(const std::vector<int>& dst, Runs* r) {
 
 // passes for the fused unitaries: consecutive parts whose slots (plus the two
 // lowest slots) fit a tile of 2^12 amplitudes, at most kFusedMaxOps per pass
+// pass shape: unitaries per state pass and tile bits (hs_set_fused_shape)
+std::atomic<int> g_fused_ops{kFusedMaxOps}, g_fused_bits{12};
+
 int plan_fused(int n, const std::vector<int>& q2s, const std::vector<PartLocal>& parts,
                int precision, std::vector<FusedPass>* out) {
   out->clear();
-  const int mmax = std::min(n, 12);
+  const int mmax = std::min(n, g_fused_bits.load());
+  const int max_ops = g_fused_ops.load();
   size_t p = 0;
   while (p < parts.size()) {
     std::vector<int> slots = {0, 1};
     size_t e = p;
-    while (e < parts.size() && int(e - p) < kFusedMaxOps) {
+    while (e < parts.size() && int(e - p) < max_ops) {
       std::vector<int> s2 = slots;
       for (int j = 0; j < kFusedBits; ++j) {
         const int sl = q2s[parts[e].qubits[j]];
@@ -198,6 +204,56 @@ int hs_fused_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_o
   HS_CUDA(cudaStreamSynchronize(s));
   if (err) return set_error(HS_E_TIMEOUT, "a tensor-core wait in K4 timed out");
   return HS_OK;
+}
+
+int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int precision,
+                   void* stream) {
+  if (!st || !st->amp) return set_error(HS_E_INVALID, "null or destroyed state");
+  if (st->dtype != HS_DTYPE_C64)
+    return set_error(HS_E_UNSUPPORTED, "the fused form runs on complex64 states");
+  if (st->n < 10) return set_error(HS_E_UNSUPPORTED, "the fused form needs at least 10 qubits");
+  if (!u || !qubits) return set_error(HS_E_INVALID, "null unitary or qubit list");
+  if (precision != HS_FUSED_BF16X3 && precision != HS_FUSED_BF16X1)
+    return set_error(HS_E_INVALID, "unknown precision %d", precision);
+  std::vector<PartLocal> parts(1);
+  for (int j = 0; j < kFusedBits; ++j) {
+    const int q = qubits[j];
+    if (q < 0 || q >= st->n) return set_error(HS_E_INVALID, "qubit %d out of range", q);
+    for (int k = 0; k < j; ++k)
+      if (qubits[k] == q) return set_error(HS_E_INVALID, "qubit %d repeated", q);
+    parts[0].qubits[j] = q;
+  }
+  const cudaStream_t s = S(stream);
+  DevBuf d_u, d_a, d_err;
+  d_u.s = d_a.s = d_err.s = s;
+  HS_CUDA(cudaMallocAsync(&d_u.p, sizeof(double2) * kFusedDim * kFusedDim, s));
+  HS_CUDA(cudaMallocAsync(&d_a.p, kFusedABytes, s));
+  HS_CUDA(cudaMallocAsync(&d_err.p, sizeof(int), s));
+  HS_CUDA(cudaMemcpyAsync(d_u.p, u, sizeof(double2) * kFusedDim * kFusedDim,
+                          cudaMemcpyHostToDevice, s));
+  HS_CUDA(cudaMemsetAsync(d_err.p, 0, sizeof(int), s));
+  HS_TRY(launch_pack(static_cast<const double2*>(d_u.p), 1, d_a.p, s));
+  std::vector<FusedPass> passes;
+  HS_TRY(plan_fused(st->n, st->q2s, parts, precision, &passes));
+  {
+    TimedRegion tr(s);
+    for (const auto& P : passes) {
+      HS_TRY(launch_fused(st->amp, P, d_a.p, static_cast<int*>(d_err.p), s));
+      count_pass(P.nops);
+    }
+  }
+  int err = 0;
+  HS_CUDA(cudaMemcpyAsync(&err, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HS_CUDA(cudaStreamSynchronize(s));
+  if (err) return set_error(HS_E_TIMEOUT, "a tensor-core wait in K4 timed out");
+  return HS_OK;
+}
+
+int hs_set_fused_shape(int max_ops_per_pass, int tile_bits) {
+  if (max_ops_per_pass < 1 || max_ops_per_pass > kFusedMaxOps || tile_bits < 10 || tile_bits > 12)
+    return set_error(HS_E_INVALID, "1..%d unitaries per pass, 10..12 tile bits", kFusedMaxOps);
+  const int prev = g_fused_ops.exchange(max_ops_per_pass) * 100 + g_fused_bits.exchange(tile_bits);
+  return prev;
 }
 
 int hs_fused_compose(int num_qubits, const hs_gate* gates, const int32_t* part_offsets,

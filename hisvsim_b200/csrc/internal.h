@@ -73,6 +73,7 @@ enum OpKind : uint8_t {
 //   2q dense, uncontrolled (v -> other array):      64 + pair        (64..69)
 //   2q dense, controlled (in place):                72 + pair        (72..77)
 //   2q swap (in place):                             80 + pair        (80..85)
+//   layer of 1q dense, uncontrolled, register mask p (>= 2 bits): 96 + p
 enum TargetWhere : uint8_t { TW_NONE = 0, TW_REG = 1, TW_THR = 2, TW_OUT = 3 };
 
 struct DevOp {
@@ -170,6 +171,8 @@ struct FusedPass {
 int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, double2* d_u,
                    void* d_a, cudaStream_t s);
 int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cudaStream_t s);
+// row-major 64 x 64 unitaries (nparts of them) -> A operands (real form, BF16 hi/lo)
+int launch_pack(const double2* d_u, int nparts, void* d_a, cudaStream_t s);
 int reduce_compare(const void* a, int adtype, const void* b, int bdtype, int n, double out[4],
                    cudaStream_t s);
 int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, uint64_t count,

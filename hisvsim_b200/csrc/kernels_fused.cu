@@ -17,6 +17,24 @@
 namespace hisv {
 namespace {
 
+// The real form with (re, im) interleaved: row r = 2*po + co, column
+// k = 2*pi + ci holds Re U (co = ci), -Im U (co=0, ci=1) or Im U (co=1, ci=0)
+// of U(po, pi); stored as BF16 hi / lo in the K-major operand layout.  Thread
+// j of 64 handles every 64th element.
+__device__ void pack_real_form(const double2* __restrict__ U, uint8_t* __restrict__ ao, int j) {
+  for (int e = j; e < 128 * 128; e += kFusedDim) {
+    const int r = e >> 7, c = e & 127;
+    const double2 u = U[(r >> 1) * kFusedDim + (c >> 1)];
+    const int co = r & 1, ci = c & 1;
+    const double x = co == ci ? u.x : (co == 0 ? -u.y : u.y);
+    const __nv_bfloat16 hi = __double2bfloat16(x);
+    const __nv_bfloat16 lo = __double2bfloat16(x - double(__bfloat162float(hi)));
+    const uint32_t off = tc::kmajor_off(uint32_t(r), uint32_t(c), 2048u);
+    *reinterpret_cast<__nv_bfloat16*>(ao + off) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(ao + kFusedABytes / 2 + off) = lo;
+  }
+}
+
 // ---- K5: compose each part's unitary in FP64 --------------------------------
 // One CTA per part, thread j owns column j of U (the image of basis state j);
 // U lives row-major in shared memory so that a warp's accesses are contiguous.
@@ -66,25 +84,19 @@ __global__ void __launch_bounds__(64) k5_compose(const FusedGate* __restrict__ g
     double2* uo = u_out + size_t(part) * kFusedDim * kFusedDim;
     for (int i = 0; i < kFusedDim; ++i) uo[i * kFusedDim + j] = U[i * kFusedDim + j];
   }
-  // The real form with (re, im) interleaved: row r = 2*po + co, column
-  // k = 2*pi + ci holds Re U (co = ci), -Im U (co=0, ci=1) or Im U (co=1, ci=0)
-  // of U(po, pi); stored as BF16 hi / lo in the K-major operand layout.
-  uint8_t* ao = a_out + size_t(part) * kFusedABytes;
-  for (int e = j; e < 128 * 128; e += kFusedDim) {
-    const int r = e >> 7, c = e & 127;
-    const double2 u = U[(r >> 1) * kFusedDim + (c >> 1)];
-    const int co = r & 1, ci = c & 1;
-    const double x = co == ci ? u.x : (co == 0 ? -u.y : u.y);
-    const __nv_bfloat16 hi = __double2bfloat16(x);
-    const __nv_bfloat16 lo = __double2bfloat16(x - double(__bfloat162float(hi)));
-    const uint32_t off = tc::kmajor_off(uint32_t(r), uint32_t(c), 2048u);
-    *reinterpret_cast<__nv_bfloat16*>(ao + off) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(ao + kFusedABytes / 2 + off) = lo;
-  }
+  pack_real_form(U, a_out + size_t(part) * kFusedABytes, j);
+}
+
+// A user-supplied unitary (row-major 64 x 64 per part) packed the same way
+__global__ void __launch_bounds__(64) k5_pack(const double2* __restrict__ u,
+                                              uint8_t* __restrict__ a_out) {
+  pack_real_form(u + size_t(blockIdx.x) * kFusedDim * kFusedDim,
+                 a_out + size_t(blockIdx.x) * kFusedABytes, threadIdx.x);
 }
 
 // ---- K4: apply fused unitaries to complex64 tiles on the tensor cores --------
 constexpr int kK4Threads = 256;
+constexpr uint32_t kK4TmemCols = 64;  // FP32 accumulator: 128 lanes x N <= 64 columns
 constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before giving up
 
 __device__ __forceinline__ uint64_t dep(uint64_t x, const Runs& r) {
@@ -111,7 +123,7 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 //                [tile buffers: 2 x 2^m complex64][tables][mbarrier][TMEM address]
 // The next tile streams into the second buffer (cp.async, 16-byte chunks of two
 // amplitudes) while the current one is processed.
-__global__ void __launch_bounds__(kK4Threads, 1)
+__global__ void __launch_bounds__(kK4Threads, 2)
     k4_fused(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
              const uint8_t* __restrict__ a_all, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t sm[];
@@ -127,8 +139,9 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   float* buf0 = reinterpret_cast<float*>(sBl + N * 256);  // interleaved (re, im)
   float* buf1 = buf0 + 2 * T;
   uint16_t* dp = reinterpret_cast<uint16_t*>(buf1 + 2 * T);  // [nops][64]
-  uint16_t* dn = dp + kFusedMaxOps * 64;                      // [nops][256]
-  uint64_t* gk = reinterpret_cast<uint64_t*>(dn + kFusedMaxOps * 256);  // [8] chunk-row offsets
+  uint16_t* dn = dp + P.nops * 64;                            // [nops][N]
+  uint64_t* gk = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(dn + P.nops * N) + 7) & ~uintptr_t(7));  // chunk-row offsets
   uint64_t* mbar = gk + 8;
   uint32_t* tmem_base = reinterpret_cast<uint32_t*>(mbar + 1);
 
@@ -149,7 +162,7 @@ __global__ void __launch_bounds__(kK4Threads, 1)
       uint32_t x = 0, bit = 0;
       for (int b = 0; b < m; ++b)
         if (!((pmask >> b) & 1)) x |= uint32_t((nn >> bit++) & 1) << b;
-      dn[o * 256 + nn] = uint16_t(tswz(x));
+      dn[o * N + nn] = uint16_t(tswz(x));
     }
   }
   // chunk c = t + r*256 holds tile indices 2c, 2c+1 (tile bit 0 is slot 0);
@@ -158,7 +171,7 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   for (int r = t; r < rows; r += kK4Threads) gk[r] = dep(uint64_t(r) * kK4Threads * 2, P.tile);
   if (t == 0) tc::mbar_init(mbar, 1);
   if (warp == 0) {
-    tc::tmem_alloc(tmem_base, 256);
+    tc::tmem_alloc(tmem_base, kK4TmemCols);
     tc::tmem_relinquish();
   }
   tc::fence_proxy_async_smem();
@@ -195,7 +208,7 @@ __global__ void __launch_bounds__(kK4Threads, 1)
       // run over consecutive columns, i.e. over the low tile bits.
       for (int item = t; item < N * 16; item += kK4Threads) {
         const int kb = item >> lgN, nn = item & (N - 1);
-        const uint32_t col = dn[o * 256 + nn];
+        const uint32_t col = dn[o * N + nn];
         uint32_t hw[4], lw[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -255,7 +268,7 @@ __global__ void __launch_bounds__(kK4Threads, 1)
           tc::tmem_ld16(tmem + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
           // the 16 column positions are the same for every lane: read them as
           // eight broadcast 32-bit words
-          const uint32_t* cw = reinterpret_cast<const uint32_t*>(dn + o * 256 + c0);
+          const uint32_t* cw = reinterpret_cast<const uint32_t*>(dn + o * N + c0);
 #pragma unroll
           for (int j = 0; j < 16; j += 2) {
             const uint32_t w = cw[j >> 1];
@@ -277,7 +290,195 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   }
   cp_async_wait0();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 256);
+  if (warp == 0) tc::tmem_dealloc(tmem, kK4TmemCols);
+}
+
+// ---- K4, one unitary per pass, pipelined across tiles -----------------------
+// Tile i's MMAs run on the tensor cores while the CTA drains tile i-1 (TMEM
+// -> shared -> global) and builds B for tile i+1; the next-but-one tile
+// streams in meanwhile.  Two TMEM accumulators and two B buffers alternate,
+// three tile buffers rotate (load / MMA source / drain).
+// Shared memory: [A 64 KiB][B0 hi|lo][B1 hi|lo][X0][X1][X2][tables][2 mbarriers][TMEM address]
+__global__ void __launch_bounds__(kK4Threads, 1)
+    k4_pipe(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
+            const uint8_t* __restrict__ a_all, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m = P.m;
+  const int T = 1 << m;
+  const int N = T >> kFusedBits;
+  const int lgN = m - kFusedBits;
+  const uint32_t bk = uint32_t(N) * 16u;
+  const uint32_t bbytes = uint32_t(N) * 256u;  // one of B hi / B lo
+  uint8_t* sA = sm;
+  uint8_t* sB = sA + kFusedABytes;               // [2][hi|lo]
+  float* X0 = reinterpret_cast<float*>(sB + 4 * bbytes);
+  uint16_t* dp = reinterpret_cast<uint16_t*>(X0 + 3 * 2 * T);  // [64]
+  uint16_t* dn = dp + 64;                                       // [N]
+  uint64_t* gk = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(dn + N) + 7) & ~uintptr_t(7));
+  uint64_t* mbar = gk + 8;  // [2]
+  uint32_t* tmem_base = reinterpret_cast<uint32_t*>(mbar + 2);
+
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a_all + size_t(P.part[0]) * kFusedABytes);
+    uint4* dst = reinterpret_cast<uint4*>(sA);
+    for (int i = t; i < kFusedABytes / 16; i += kK4Threads) dst[i] = src[i];
+  }
+  uint32_t pmask = 0;
+  for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[0][b];
+  for (int p = t; p < 64; p += kK4Threads) {
+    uint32_t x = 0;
+    for (int b = 0; b < kFusedBits; ++b) x |= uint32_t((p >> b) & 1) << P.pbits[0][b];
+    dp[p] = uint16_t(tswz(x));
+  }
+  for (int nn = t; nn < N; nn += kK4Threads) {
+    uint32_t x = 0, bit = 0;
+    for (int b = 0; b < m; ++b)
+      if (!((pmask >> b) & 1)) x |= uint32_t((nn >> bit++) & 1) << b;
+    dn[nn] = uint16_t(tswz(x));
+  }
+  const int chunks = T / 2, rows = chunks / kK4Threads;
+  for (int r = t; r < rows; r += kK4Threads) gk[r] = dep(uint64_t(r) * kK4Threads * 2, P.tile);
+  if (t == 0) {
+    tc::mbar_init(&mbar[0], 1);
+    tc::mbar_init(&mbar[1], 1);
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_base, 2 * kK4TmemCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_base;
+  const uint64_t gt = dep(uint64_t(t) * 2, P.tile);
+  const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
+  const int nprod = P.precision == 1 ? 1 : 3;
+  uint32_t phase[2] = {0, 0};
+  bool pend[2] = {false, false};  // an MMA group committed to mbar[b] and not yet awaited
+  bool failed = false;
+  auto xbuf = [&](int i) { return X0 + (i % 3) * 2 * T; };
+  auto issue_load = [&](uint64_t tl, float* dst) {
+    const uint64_t gb = dep(tl, P.outer);
+    const uint32_t ds = tc::smem_u32(dst);
+    for (int r = 0; r < rows; ++r)
+      cp_async16(ds + tswz(2u * uint32_t(t + r * kK4Threads)) * 8u, sv + gb + gt + gk[r]);
+  };
+  // tiles of this CTA: blockIdx.x + i * gridDim.x, i < cnt
+  const uint64_t cnt =
+      blockIdx.x < P.ntiles ? (P.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto tile_of = [&](uint64_t i) { return blockIdx.x + i * gridDim.x; };
+  if (cnt > 0) issue_load(tile_of(0), xbuf(0));
+  cp_async_commit();
+  if (cnt > 1) issue_load(tile_of(1), xbuf(1));
+  cp_async_commit();
+
+  // drain tile j: TMEM accumulator j%2 -> X(j) -> global
+  auto drain = [&](uint64_t j) -> bool {
+    const int b = int(j & 1);
+    const bool ok = tc::mbar_wait(&mbar[b], phase[b], kWaitLimit);
+    if (__syncthreads_or(!ok)) return false;
+    phase[b] ^= 1u;
+    pend[b] = false;
+    tc::tc_fence_after();
+    float* X = xbuf(int(j % 3));
+    {
+      const int quad = warp & 3, half = warp >> 2;
+      const int r = quad * 32 + lane;
+      const int comp = r & 1;
+      const uint32_t prow = dp[r >> 1];
+      const int per_half = N / 2 < 16 ? 16 : N / 2;
+      const int c_begin = half * per_half;
+      const int c_end = c_begin + per_half < N ? c_begin + per_half : N;
+      for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
+        float d[16];
+        tc::tmem_ld16(tmem + uint32_t(b) * kK4TmemCols + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(dn + c0);
+#pragma unroll
+        for (int q = 0; q < 16; q += 2) {
+          const uint32_t w = cw[q >> 1];
+          X[2 * (prow ^ (w & 0xffffu)) + comp] = d[q];
+          X[2 * (prow ^ (w >> 16)) + comp] = d[q + 1];
+        }
+      }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    const uint64_t gbase = dep(tile_of(j), P.outer);
+    for (int r = 0; r < rows; ++r) {
+      const uint4 v = *reinterpret_cast<const uint4*>(X + 2 * tswz(2u * uint32_t(t + r * kK4Threads)));
+      __stcs(reinterpret_cast<uint4*>(sv + gbase + gt + gk[r]), v);
+    }
+    __syncthreads();  // X(j) may be refilled
+    return true;
+  };
+
+  for (uint64_t i = 0; i < cnt; ++i) {
+    cp_async_wait1();  // tile i has landed (tile i+1 may be in flight)
+    __syncthreads();
+    const float* X = xbuf(int(i % 3));
+    uint8_t* bh = sB + (i & 1) * 2 * bbytes;
+    uint8_t* bl = bh + bbytes;
+    for (int item = t; item < N * 16; item += kK4Threads) {
+      const int kb = item >> lgN, nn = item & (N - 1);
+      const uint32_t col = dn[nn];
+      uint32_t hw[4], lw[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float2 x = *reinterpret_cast<const float2*>(X + 2 * (dp[4 * kb + q] ^ col));
+        const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(x.x - hf.x, x.y - hf.y);
+        hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+        lw[q] = *reinterpret_cast<const uint32_t*>(&l);
+      }
+      const uint32_t off = tc::kmajor_off(uint32_t(nn), uint32_t(kb * 8), bk);
+      *reinterpret_cast<uint4*>(bh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(bl + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+    tc::fence_proxy_async_smem();
+    tc::tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::tc_fence_after();
+      const uint32_t a0 = tc::smem_u32(sA);
+      const uint32_t bhs = tc::smem_u32(bh), bls = tc::smem_u32(bl);
+      const uint32_t d = tmem + uint32_t(i & 1) * kK4TmemCols;
+      uint32_t acc = 0;
+      for (int prod = 0; prod < nprod; ++prod) {
+        const uint32_t abase = a0 + (prod == 2 ? uint32_t(kFusedABytes / 2) : 0u);
+        const uint32_t bbase = prod == 1 ? bls : bhs;
+        for (int s = 0; s < 8; ++s) {
+          const uint64_t ad = tc::smem_desc(abase + uint32_t(s) * 2u * 2048u, 2048u, 128u);
+          const uint64_t bd = tc::smem_desc(bbase + uint32_t(s) * 2u * bk, bk, 128u);
+          tc::mma_bf16(d, ad, bd, idesc, acc);
+          acc = 1;
+        }
+      }
+      tc::mma_commit(&mbar[i & 1]);
+    }
+    pend[i & 1] = true;
+    // while tile i multiplies: drain tile i-1, then refill its buffer with tile i+2
+    if (i > 0 && !drain(i - 1)) {
+      failed = true;
+      break;
+    }
+    if (i + 2 < cnt) issue_load(tile_of(i + 2), xbuf(int((i + 2) % 3)));
+    cp_async_commit();
+  }
+  if (!failed && cnt > 0 && !drain(cnt - 1)) failed = true;
+  if (failed) {
+    if (t == 0) atomicExch(err, 1);
+    // the MMAs still in flight complete (or time out) before TMEM is freed
+    for (int b = 0; b < 2; ++b)
+      if (pend[b]) tc::mbar_wait(&mbar[b], phase[b], kWaitLimit);
+  }
+  cp_async_wait0();
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4TmemCols);
 }
 
 }  // namespace
@@ -297,6 +498,13 @@ int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, 
   return HS_OK;
 }
 
+int launch_pack(const double2* d_u, int nparts, void* d_a, cudaStream_t s) {
+  if (nparts <= 0) return HS_OK;
+  k5_pack<<<nparts, kFusedDim, 0, s>>>(d_u, static_cast<uint8_t*>(d_a));
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+
 int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
@@ -304,14 +512,37 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     attr = true;
   }
   const int T = 1 << P.m, N = T >> kFusedBits;
-  const size_t smem = size_t(P.nops) * kFusedABytes + size_t(N) * 512 + size_t(T) * 16 +
-                      2 * (kFusedMaxOps * 64 + kFusedMaxOps * 256) + 8 * 8 + 8 + 8 + 16;
+  // A operands, B hi/lo, two tile buffers, the dp/dn tables, chunk offsets
+  // (8-byte aligned), mbarrier, TMEM address
+  const size_t tables = (size_t(P.nops) * (64 + N) * 2 + 7) & ~size_t(7);
+  const size_t smem = size_t(P.nops) * kFusedABytes + size_t(N) * 512 + size_t(T) * 16 + tables +
+                      8 * 8 + 8 + 8 + 16;
   if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 pass needs %zu B of shared memory", smem);
   int sms = 148;
-  int dev = 0;
+  int dev = 0, per_sm = 1;
   HS_CUDA(cudaGetDevice(&dev));
   HS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int grid = int(P.ntiles < uint64_t(sms) ? P.ntiles : uint64_t(sms));
+  HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k4_fused, kK4Threads, smem));
+  if (per_sm < 1) return set_error(HS_E_UNSUPPORTED, "K4 pass does not fit an SM");
+  const uint64_t want = uint64_t(sms) * uint64_t(per_sm);
+  const int grid = int(P.ntiles < want ? P.ntiles : want);
+  if (P.nops == 1) {
+    // pipelined form: A, two B buffers, three tile buffers, tables
+    static bool pattr = false;
+    if (!pattr) {
+      HS_CUDA(cudaFuncSetAttribute(k4_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+      pattr = true;
+    }
+    const size_t psmem = size_t(kFusedABytes) + size_t(N) * 1024 + size_t(T) * 24 +
+                         ((size_t(64 + N) * 2 + 7) & ~size_t(7)) + 8 * 8 + 16 + 16;
+    if (psmem <= 227 * 1024) {
+      const int pgrid = int(P.ntiles < uint64_t(sms) ? P.ntiles : uint64_t(sms));
+      k4_pipe<<<pgrid, kK4Threads, psmem, s>>>(static_cast<float2*>(amp), P,
+                                               static_cast<const uint8_t*>(d_a), d_err);
+      HS_CUDA(cudaGetLastError());
+      return HS_OK;
+    }
+  }
   k4_fused<<<grid, kK4Threads, smem, s>>>(static_cast<float2*>(amp), P,
                                           static_cast<const uint8_t*>(d_a), d_err);
   HS_CUDA(cudaGetLastError());

@@ -196,6 +196,14 @@ int hs_fused_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_o
  * (row-major, row = output basis index); out_qubits: num_parts x 6, the qubit
  * of each local bit (bit j = j-th lowest slot; parts smaller than six qubits
  * are padded with the lowest other qubits). */
+/* Apply one given 64x64 unitary (row-major, interleaved re/im doubles; local
+ * index bit j = qubits[j]) to a complex64 state with K4: the form of
+ * gather_and_execute_on for a part whose unitary the caller already has. */
+int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int precision,
+                   void* stream);
+/* Shape of the fused passes: unitaries applied per state pass (1..2) and
+ * tile bits (10..12).  Returns the previous shape as ops * 100 + bits. */
+int hs_set_fused_shape(int max_ops_per_pass, int tile_bits);
 int hs_fused_compose(int num_qubits, const hs_gate* gates, const int32_t* part_offsets,
                      int num_parts, double* out_u, int32_t* out_qubits);
 /* out = {Re<a|b>, Im<a|b>, max|a-b|, <b|b>} in FP64 for states of any two

@@ -103,3 +103,48 @@ def test_fused_errors():
     big = [Gate("X", (q,)) for q in range(7)]
     with pytest.raises(abi.HisvError):
         abi.State(12, abi.C64).run_fused(to_records(big), np.array([0, 7]))
+
+
+@pytest.mark.parametrize("shape", [(1, 10), (1, 11), (1, 12), (2, 11), (2, 12)])
+def test_fused_pass_shapes(port, shape):
+    """Every pass shape (unitaries per pass, tile bits) gives the same result;
+    (1, 11) runs two CTAs per SM."""
+    n = 15
+    gates = circuits.random_u3_cz(n, 8, 17)
+    parts = partition.partition_acyclic(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    prev = abi.set_fused_shape(*shape)
+    try:
+        st = abi.State(n, abi.C64)
+        st.run_fused(rec, offs, 0)
+        got = st.amplitudes().astype(complex)
+    finally:
+        abi.set_fused_shape(prev // 100, prev % 100)
+    assert 1 - fid(want, got) <= 1e-8
+    assert np.abs(got - want).max() <= 1e-5
+
+
+def test_fused_apply_given_unitary():
+    """hs_fused_apply with a random 64x64 unitary on scattered qubits, against
+    numpy on the complex128 amplitudes."""
+    n = 12
+    rng = np.random.default_rng(4)
+    z = rng.normal(size=(64, 64)) + 1j * rng.normal(size=(64, 64))
+    u, _ = np.linalg.qr(z)
+    qubits = [11, 0, 5, 3, 9, 7]
+    st = abi.State(n, abi.C64)
+    gates = circuits.random_u3_cz(n, 3, 8)
+    for g in gates:
+        st.apply(g)
+    before = st.amplitudes().astype(complex)
+    st.fused_apply(u, qubits)
+    got = st.amplitudes().astype(complex)
+    # numpy: axis for qubit q of a C-ordered reshape is n-1-q
+    psi = before.reshape([2] * n)
+    axes = [n - 1 - q for q in qubits][::-1]  # U index bit 5 first
+    moved = np.moveaxis(psi, axes, range(6)).reshape(64, -1)
+    out = (u @ moved).reshape([2] * 6 + [2] * (n - 6))
+    want = np.moveaxis(out, range(6), axes).reshape(-1)
+    assert 1 - fid(want, got) <= 1e-8
+    assert np.abs(got - want).max() <= 1e-5

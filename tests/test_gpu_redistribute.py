@@ -116,7 +116,7 @@ def test_project_matches_numpy(mode, dtype):
     """hs_project (state_vector.hpp:829-894) against a numpy restatement, on a
     state whose slots are permuted (qubit q not at slot q)."""
     n = 9
-    gates = circuits.random_layered(n, 6, 31)
+    gates = circuits.random_u3_cz(n, 6, 31)
     st = abi.State(n, dtype)
     st.set_basis(0)
     for g in gates:
@@ -134,11 +134,19 @@ def test_project_matches_numpy(mode, dtype):
     wp = float(np.sum(np.abs(want) ** 2))
     tol = 1e-12 if dtype == abi.C128 else 1e-5
     assert p == pytest.approx(wp, rel=tol, abs=tol)
+    assert wp > 1e-3  # a generic state: the projected part is not empty
     want = want / (np.sqrt(wp) if mode == 0 else wp if mode == 1 else 1.0)
     assert sub.n == n - 3
     assert np.abs(sub.amplitudes() - want).max() <= tol * max(1.0, np.abs(want).max())
     if mode == 0:
         assert sub.norm2() == pytest.approx(1.0, abs=tol)
+
+
+def test_project_of_an_empty_part_is_left_unnormalised():
+    st = abi.State(5)
+    st.set_basis(0b00101)
+    sub, p = st.project([0], [0])  # qubit 0 is 1 with certainty
+    assert p == 0.0 and np.abs(sub.amplitudes()).max() == 0.0
 
 
 def test_project_rejects_bad_arguments():
