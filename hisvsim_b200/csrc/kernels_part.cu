@@ -124,18 +124,6 @@ __device__ __forceinline__ void d1c(V (&v)[1 << R], const double2* __restrict__ 
   }
 }
 
-// a layer of uncontrolled dense 2x2 gates on the register bits in mask M
-// (distinct qubits, applied in increasing bit order; four coefficients each)
-template <int R, int M, typename V>
-__device__ __forceinline__ void dlayer(V (&v)[1 << R], const double2* __restrict__ c) {
-  int k = 0;
-  if constexpr ((M & 1) && R > 0) d1c<R, 0>(v, c + 4 * k++, 0u, true);
-  if constexpr ((M & 2) && R > 1) d1c<R, 1>(v, c + 4 * k++, 0u, true);
-  if constexpr ((M & 4) && R > 2) d1c<R, 2>(v, c + 4 * k++, 0u, true);
-  if constexpr ((M & 8) && R > 3) d1c<R, 3>(v, c + 4 * k++, 0u, true);
-  (void)k;
-}
-
 // sign flip of the elements whose register bits cover mask M (sm = 0 or sign bit)
 template <int R, int M, typename V>
 __device__ __forceinline__ void dneg(V (&v)[1 << R], uint32_t sm) {
@@ -275,8 +263,6 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
   case (J): if constexpr ((J) < R) d1c<R, J>(v, c, 0u, true); break;
 #define D2(P, JA, JB) \
   case 64 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, 0u, true); break;
-#define LY(M) \
-  case 96 + (M): if constexpr ((M) < (1 << R)) dlayer<R, M>(v, c); break;
   switch (op.code) {
     D1(0) D1(1) D1(2) D1(3)
     D2(0, 0, 1) D2(1, 0, 2) D2(2, 0, 3) D2(3, 1, 2) D2(4, 1, 3) D2(5, 2, 3)
@@ -288,10 +274,8 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
     case 48: ddiag<R>(v, op, c, thr, gbase, ok); break;
     C2(0, 0, 1) C2(1, 0, 2) C2(2, 0, 3) C2(3, 1, 2) C2(4, 1, 3) C2(5, 2, 3)
     SW(0, 0, 1) SW(1, 0, 2) SW(2, 0, 3) SW(3, 1, 2) SW(4, 1, 3) SW(5, 2, 3)
-    LY(3) LY(5) LY(6) LY(7) LY(9) LY(10) LY(11) LY(12) LY(13) LY(14) LY(15)
     default: break;
   }
-#undef LY
 #undef D1
 #undef D2
 #undef C1
@@ -366,6 +350,7 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
   const uint32_t t = threadIdx.x;
   const uint32_t nthr = blockDim.x;
   const uint32_t tile_bytes = uint32_t(sizeof(V)) << P.m;
+  unsigned char* buf[2] = {smem_raw, smem_raw + tile_bytes};
   uint64_t* s_gchunk = reinterpret_cast<uint64_t*>(smem_raw + 2 * tile_bytes);
   // chunk c = t + k*nthr; its first tile index is c << SH.  The bits of t and
   // of k*nthr are disjoint, so deposit(c << SH) = deposit(t << SH) + deposit(k*nthr << SH).
@@ -375,8 +360,8 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
     s_gchunk[k] = deposit(uint64_t(k) * nthr << M::SH, P.tile);
   __syncthreads();
   const uint64_t gt = deposit(uint64_t(t) << M::SH, P.tile);
-  const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(smem_raw));
-  const uint32_t sb1 = sb0 + tile_bytes;
+  const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(buf[0]));
+  const uint32_t sb1 = uint32_t(__cvta_generic_to_shared(buf[1]));
 
   uint64_t tile = blockIdx.x;
   if (tile < P.ntiles)
@@ -391,9 +376,7 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
     cp_async_commit();
     cp_async_wait<1>();  // this tile's copies (all but the newest group) have landed
     __syncthreads();
-    // derived from smem_raw by arithmetic (not picked from an array), so the
-    // compiler keeps shared-memory instructions for every tile access
-    unsigned char* A = smem_raw + (it & 1) * tile_bytes;
+    unsigned char* A = buf[it & 1];
     const uint64_t gbase = deposit(tile, P.outer);
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];

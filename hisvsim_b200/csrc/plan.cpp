@@ -179,35 +179,6 @@ void emit_op(const SlotGate& sg, const Layout& L, PartProgram* P) {
   P->ops[P->nops++] = op;
 }
 
-// Several uncontrolled dense one-qubit gates on distinct register positions,
-// applied as one op (they act on different qubits, so their order is free):
-// one dispatch and one pass over the registers instead of one per gate.
-// mats[j] is the gate on register position j (has[j]).
-void emit_layer(const cplx (&mats)[kRegBits][4], const bool (&has)[kRegBits], PartProgram* P) {
-  int mask = 0, count = 0, last = 0;
-  for (int j = 0; j < kRegBits; ++j)
-    if (has[j]) {
-      mask |= 1 << j;
-      ++count;
-      last = j;
-    }
-  if (count == 0) return;
-  DevOp op;
-  std::memset(&op, 0, sizeof(op));
-  op.kind = OP1_DENSE;
-  op.coef = uint16_t(P->ncoef);
-  for (int j = 0; j < kRegBits; ++j)
-    if (has[j])
-      for (int k = 0; k < 4; ++k) {
-        P->coef[P->ncoef].x = mats[j][k].real();
-        P->coef[P->ncoef].y = mats[j][k].imag();
-        ++P->ncoef;
-      }
-  op.ja = uint8_t(last);
-  op.code = uint8_t(count == 1 ? last : 96 + mask);
-  P->ops[P->nops++] = op;
-}
-
 }  // namespace
 
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
@@ -344,57 +315,7 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       for (int b = 0; b < kMaxTileBits; ++b) L.regpos_of_tbit[b] = -1;
       for (int j = 0; j < R; ++j) L.regpos_of_tbit[regs[j]] = j;
       gd.first_op = uint16_t(P->nops);
-      // uncontrolled dense one-qubit gates wait as pending 2x2 matrices per
-      // register position (products of consecutive ones on the same qubit);
-      // an op touching a position first flushes the pending gates there, and
-      // what remains is flushed as one layer op at the end of the group
-      cplx pend[kRegBits][4];
-      bool has[kRegBits] = {false, false, false, false};
-      auto flush = [&](int mask) {
-        bool sel[kRegBits];
-        bool any = false;
-        for (int j = 0; j < kRegBits; ++j) {
-          sel[j] = has[j] && ((mask >> j) & 1);
-          any |= sel[j];
-        }
-        if (!any) return;
-        emit_layer(pend, sel, P);
-        for (int j = 0; j < kRegBits; ++j)
-          if (sel[j]) has[j] = false;
-      };
-      for (size_t x : members) {
-        const SlotGate& g = sgs[x];
-        if (!g.diag && g.g->nt == 1 && g.nc == 0) {
-          uint8_t w, j;
-          locate(L, g.ts[0], &w, &j);
-          const cplx* m = g.g->m;
-          if (has[j]) {  // m * pend[j]
-            const cplx a[4] = {pend[j][0], pend[j][1], pend[j][2], pend[j][3]};
-            pend[j][0] = m[0] * a[0] + m[1] * a[2];
-            pend[j][1] = m[0] * a[1] + m[1] * a[3];
-            pend[j][2] = m[2] * a[0] + m[3] * a[2];
-            pend[j][3] = m[2] * a[1] + m[3] * a[3];
-          } else {
-            for (int k = 0; k < 4; ++k) pend[j][k] = m[k];
-            has[j] = true;
-          }
-          continue;
-        }
-        int touch = 0;
-        for (int i = 0; i < g.g->nt; ++i) {
-          uint8_t w, pos;
-          locate(L, g.ts[i], &w, &pos);
-          if (w == TW_REG) touch |= 1 << pos;
-        }
-        for (int i = 0; i < g.nc; ++i) {
-          uint8_t w, pos;
-          locate(L, g.cs[i], &w, &pos);
-          if (w == TW_REG) touch |= 1 << pos;
-        }
-        flush(touch);
-        emit_op(g, L, P);
-      }
-      flush((1 << kRegBits) - 1);
+      for (size_t x : members) emit_op(sgs[x], L, P);
       gd.num_ops = uint16_t(P->nops - gd.first_op);
       remaining = rest;
     }
