@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--tile-qubits", type=int, default=11, help="K1 tile bits (0 = automatic)")
     ap.add_argument("--no-fused", action="store_true", help="skip the precision form")
+    ap.add_argument("--fused-shape", default="",
+                    help="unitaries per pass and tile bits of the precision form, e.g. 2,12")
     ap.add_argument("--no-fidelity", action="store_true", help="skip the 1-F check")
     ap.add_argument("--no-batch", action="store_true", help="skip the batching form")
     ap.add_argument("--batch-instances", type=int, default=512)
@@ -263,6 +265,7 @@ def batch_form(args, abi, peak_gbs, pg, device):
             "hbm_frac": st["bytes_per_run"] / t_run / 1e9 / peak_gbs,
             "bytes_per_run": st["bytes_per_run"], "work_items": st["items"],
             "tuned": {"tile_cap": cap, "ctas_per_sm": ctas, "best_ms": tune_ms,
+                      "tiles_per_item": st["tiles_per_item"], "low_keep": st["low_keep"],
                       "caps_by_qubits": {int(n): int(c) for n, c in zip(ns, caps)}},
             "max_hc_err_per_edge": worst, "checked_instances": check,
             "plain_c128_sequential_s": t_plain,
@@ -371,6 +374,8 @@ def main():
     fused = None
     fused_host = None
     if not args.no_fused:
+        if args.fused_shape:
+            abi.set_fused_shape(*[int(x) for x in args.fused_shape.split(",")])
         fparts = partition.partition_acyclic(gates, 6)
         frec, foffs = part_offsets(partition.parts_to_gates(gates, fparts))
         stf = abi.State(n, abi.C64)

@@ -75,6 +75,7 @@ SIGNATURES = {
     "hs_batch_run": [_vp, _vp, _dp],
     "hs_batch_stats": [_vp, _vp],
     "hs_batch_set_chunk": [_vp, _i],
+    "hs_batch_set_low_keep": [_vp, _i],
     "hs_batch_tile_caps": [_vp, _vp],
     "hs_batch_state": [_vp, _i, _vp],
     "hs_batch_destroy": [_vp],
@@ -503,6 +504,9 @@ class QaoaBatch:
     def set_chunk(self, tiles_per_item: int):
         check(lib().hs_batch_set_chunk(self.h, tiles_per_item))
 
+    def set_low_keep(self, low: int):
+        check(lib().hs_batch_set_low_keep(self.h, low))
+
     def tune(self):
         cap, ctas, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
         check(lib().hs_batch_tune(self.h, ctypes.byref(cap), ctypes.byref(ctas), ctypes.byref(ms)))
@@ -515,10 +519,10 @@ class QaoaBatch:
         return out, ms.value
 
     def stats(self):
-        s = np.zeros(6, dtype=np.int64)
+        s = np.zeros(7, dtype=np.int64)
         check(lib().hs_batch_stats(self.h, _ptr(s)))
         return dict(zip(["items", "steps", "bytes_per_run", "tile_cap", "ctas_per_sm",
-                         "tiles_per_item"], s.tolist()))
+                         "tiles_per_item", "low_keep"], s.tolist()))
 
     def tile_caps(self) -> np.ndarray:
         caps = np.zeros(self.count, dtype=np.int32)

@@ -16,6 +16,7 @@ struct hs_batch {
   std::vector<std::vector<std::pair<int, int>>> edges;
   std::vector<double> gammas, betas;
   int tile_cap = kBatchMaxTileBits, ctas_per_sm = 6, chunk = 8;
+  int low_keep = 3;  // lowest qubits kept in every later pass's tile (contiguous runs)
   int cap_of_n[kBatchMaxQubits + 1] = {};  // per qubit count; 0 = tile_cap
   void* pool = nullptr;
   std::vector<uint64_t> offset;  // amplitude offset of each instance in the pool
@@ -72,7 +73,7 @@ void runs(const std::vector<int>& dst, Runs* r) {
 // Passes of one round for n qubits with tiles of at most `cap` bits: pass 0
 // takes qubits [0, cap) and the cost phase; later passes keep slots 0..2 for
 // contiguity and mix the next cap-3 qubits.
-int plan_passes(int n, int cap, BatchInstance* I) {
+int plan_passes(int n, int cap, int low, BatchInstance* I) {
   std::vector<std::vector<int>> tiles, targets;
   if (n <= cap) {
     std::vector<int> all;
@@ -86,15 +87,16 @@ int plan_passes(int n, int cap, BatchInstance* I) {
     targets.push_back(t0);
     int covered = cap;
     while (covered < n) {
-      const int nw = std::min(cap - 3, n - covered);
-      std::vector<int> tl = {0, 1, 2}, tg;
+      const int nw = std::min(cap - low, n - covered);
+      std::vector<int> tl, tg;
+      for (int q = 0; q < low; ++q) tl.push_back(q);
       for (int q = covered; q < covered + nw; ++q) {
         tl.push_back(q);
         tg.push_back(q);
       }
       // widen the tile with the next-lowest qubits (no gate on them in this
       // pass): fewer, larger tiles and longer contiguous runs
-      for (int q = 3; q < n && int(tl.size()) < cap; ++q)
+      for (int q = low; q < n && int(tl.size()) < cap; ++q)
         if (std::find(tl.begin(), tl.end(), q) == tl.end()) tl.push_back(q);
       std::sort(tl.begin(), tl.end());
       tiles.push_back(tl);
@@ -185,7 +187,7 @@ int build_plan(hs_batch* b) {
       I.edge_a[e] = uint8_t(b->edges[i][e].first);
       I.edge_b[e] = uint8_t(b->edges[i][e].second);
     }
-    HS_TRY(plan_passes(I.n, b->cap_of_n[I.n] ? b->cap_of_n[I.n] : b->tile_cap, &I));
+    HS_TRY(plan_passes(I.n, b->cap_of_n[I.n] ? b->cap_of_n[I.n] : b->tile_cap, b->low_keep, &I));
     I.step_base = nc;
     const int steps = I.npasses * b->p;
     nc += uint64_t(steps);
@@ -359,6 +361,19 @@ int hs_batch_set_chunk(hs_batch* b, int tiles_per_item) {
   return build_plan(b);
 }
 
+int hs_batch_set_low_keep(hs_batch* b, int low) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  if (low < 2 || low > 3) return set_error(HS_E_INVALID, "keep 2 or 3 low qubits");
+  const int old = b->low_keep;
+  b->low_keep = low;
+  const int rc = build_plan(b);
+  if (rc != HS_OK) {
+    b->low_keep = old;
+    build_plan(b);
+  }
+  return rc;
+}
+
 int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm) {
   if (!b) return set_error(HS_E_INVALID, "null batch");
   if (tile_cap < 6 || tile_cap > kBatchMaxTileBits || ctas_per_sm < 1 || ctas_per_sm > 16)
@@ -398,21 +413,25 @@ int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* be
   double best = 1e300;
   const int maxc = batch_max_ctas_per_sm();
   int bc = b->tile_cap, bt = b->ctas_per_sm, bk = b->chunk;
+  int bl = b->low_keep;
   for (int cap : {9, 10, 11})
-    for (int ctas : {std::max(1, maxc - 2), maxc})
+    for (int low : {2, 3})
       for (int chunk : {4, 16}) {
         b->chunk = chunk;
-        if (hs_batch_configure(b, cap, ctas) != HS_OK) continue;
+        b->low_keep = low;
+        if (hs_batch_configure(b, cap, maxc) != HS_OK) continue;
         double ms = 0;
         HS_TRY(timed(&ms));
         if (ms < best) {
           best = ms;
           bc = cap;
-          bt = ctas;
+          bt = maxc;
           bk = chunk;
+          bl = low;
         }
       }
   b->chunk = bk;
+  b->low_keep = bl;
   HS_TRY(hs_batch_configure(b, bc, bt));
   // 2) per qubit count, largest states first: try the other caps, keep a
   // change only if the whole batch gets at least 1% faster
@@ -459,6 +478,7 @@ int hs_batch_stats(hs_batch* b, int64_t* stats) {
   stats[3] = b->tile_cap;
   stats[4] = std::min(b->ctas_per_sm, batch_max_ctas_per_sm());
   stats[5] = b->chunk;
+  stats[6] = b->low_keep;
   return HS_OK;
 }
 

@@ -288,6 +288,9 @@ int hs_batch_set_params(hs_batch* b, const double* gammas, const double* betas);
 int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm);
 /* Tiles per work item (a dequeued chunk of one step of one instance). */
 int hs_batch_set_chunk(hs_batch* b, int tiles_per_item);
+/* Lowest qubits (2 or 3) kept in the tile of every pass after the first:
+ * 32- or 64-byte contiguous runs against one more new qubit per pass. */
+int hs_batch_set_low_keep(hs_batch* b, int low);
 /* Autotuner: times every (tile cap, CTAs per SM) candidate on the whole batch
  * and keeps the best, then refines the tile cap per qubit count (largest
  * states first), keeping a change only when the batch gets >= 1% faster. */
@@ -298,7 +301,8 @@ int hs_batch_tile_caps(hs_batch* b, int32_t* caps);
  * instance i; *ms = device time of the run between CUDA events on the
  * batch's stream, read-back of the results included (may be NULL). */
 int hs_batch_run(hs_batch* b, double* expect_out, double* ms);
-/* {work items, steps, bytes moved per run, tile cap, CTAs per SM, tiles per item} */
+/* {work items, steps, bytes moved per run, tile cap, CTAs per SM, tiles per
+ * item, lowest qubits kept in later passes' tiles} */
 int hs_batch_stats(hs_batch* b, int64_t* stats);
 /* Complex64 amplitudes of one instance (qubit order) into host memory. */
 int hs_batch_state(hs_batch* b, int instance, void* host_out);

@@ -67,6 +67,7 @@ def test_cta_schedules_agree(ctas):
     base, _ = b.run()
     b.configure(10, ctas)
     b.set_chunk(3)
+    b.set_low_keep(2)
     again, _ = b.run()
     assert np.abs(base - again).max() <= 1e-4
     b.close()
