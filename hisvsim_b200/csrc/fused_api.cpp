@@ -116,7 +116,7 @@ void runs_of(const std::vector<int>& dst, Runs* r) {
 // passes for the fused unitaries: consecutive parts whose slots (plus the two
 // lowest slots) fit a tile of 2^12 amplitudes, at most kFusedMaxOps per pass
 // pass shape: unitaries per state pass and tile bits (hs_set_fused_shape)
-std::atomic<int> g_fused_ops{kFusedMaxOps}, g_fused_bits{12};
+std::atomic<int> g_fused_ops{1}, g_fused_bits{13};
 
 int plan_fused(int n, const std::vector<int>& q2s, const std::vector<PartLocal>& parts,
                int precision, std::vector<FusedPass>* out) {
@@ -250,8 +250,9 @@ int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int pre
 }
 
 int hs_set_fused_shape(int max_ops_per_pass, int tile_bits) {
-  if (max_ops_per_pass < 1 || max_ops_per_pass > kFusedMaxOps || tile_bits < 10 || tile_bits > 12)
-    return set_error(HS_E_INVALID, "1..%d unitaries per pass, 10..12 tile bits", kFusedMaxOps);
+  if (max_ops_per_pass < 1 || max_ops_per_pass > kFusedMaxOps || tile_bits < 10 ||
+      tile_bits > (max_ops_per_pass == 1 ? 13 : 12))
+    return set_error(HS_E_INVALID, "1 unitary per pass with 10..13 tile bits, or 2 with 10..12");
   const int prev = g_fused_ops.exchange(max_ops_per_pass) * 100 + g_fused_bits.exchange(tile_bits);
   return prev;
 }

@@ -96,7 +96,8 @@ __global__ void __launch_bounds__(64) k5_pack(const double2* __restrict__ u,
 
 // ---- K4: apply fused unitaries to complex64 tiles on the tensor cores --------
 constexpr int kK4Threads = 256;
-constexpr uint32_t kK4TmemCols = 64;  // FP32 accumulator: 128 lanes x N <= 64 columns
+constexpr uint32_t kK4TmemCols = 64;     // FP32 accumulator: 128 lanes x N <= 64 columns
+constexpr uint32_t kK4DirectCols = 128;  // the direct form: N <= 128 columns, two accumulators
 constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before giving up
 
 __device__ __forceinline__ uint64_t dep(uint64_t x, const Runs& r) {
@@ -293,31 +294,33 @@ __global__ void __launch_bounds__(kK4Threads, 2)
   if (warp == 0) tc::tmem_dealloc(tmem, kK4TmemCols);
 }
 
-// ---- K4, one unitary per pass, pipelined across tiles -----------------------
-// Tile i's MMAs run on the tensor cores while the CTA drains tile i-1 (TMEM
-// -> shared -> global) and builds B for tile i+1; the next-but-one tile
-// streams in meanwhile.  Two TMEM accumulators and two B buffers alternate,
-// three tile buffers rotate (load / MMA source / drain).
-// Shared memory: [A 64 KiB][B0 hi|lo][B1 hi|lo][X0][X1][X2][tables][2 mbarriers][TMEM address]
+// ---- K4, one unitary per pass, operands straight from and to HBM ------------
+// The tile never sits in shared memory as complex64: each thread loads its
+// amplitudes from global memory (coalesced over the tile's columns), splits
+// them into the BF16 hi / lo B operands, and the epilogue moves results from
+// TMEM to global memory directly (re / im paired by a lane shuffle).  Only A
+// (64 KiB) and two B buffers live in shared memory, so tiles can be 2^13
+// amplitudes (N = 128 columns, half the tensor-core operand reads per
+// amplitude of N = 64).  Tile i's MMAs run while tile i+1's loads are in flight
+// and tile i-1 drains; two TMEM accumulators and two B buffers alternate.
+// Shared memory: [A][B0 hi|lo][B1 hi|lo][gp: 64 x u64][gn: N x u64][2 mbarriers][TMEM address]
+constexpr int kK4DirectItems = 8;  // B items per thread (N * 16 / 256 for N = 128)
+
 __global__ void __launch_bounds__(kK4Threads, 1)
-    k4_pipe(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
-            const uint8_t* __restrict__ a_all, int* __restrict__ err) {
+    k4_direct(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
+              const uint8_t* __restrict__ a_all, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t sm[];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int m = P.m;
-  const int T = 1 << m;
-  const int N = T >> kFusedBits;
+  const int N = 1 << (m - kFusedBits);
   const int lgN = m - kFusedBits;
   const uint32_t bk = uint32_t(N) * 16u;
-  const uint32_t bbytes = uint32_t(N) * 256u;  // one of B hi / B lo
+  const uint32_t bbytes = uint32_t(N) * 256u;
   uint8_t* sA = sm;
-  uint8_t* sB = sA + kFusedABytes;               // [2][hi|lo]
-  float* X0 = reinterpret_cast<float*>(sB + 4 * bbytes);
-  uint16_t* dp = reinterpret_cast<uint16_t*>(X0 + 3 * 2 * T);  // [64]
-  uint16_t* dn = dp + 64;                                       // [N]
-  uint64_t* gk = reinterpret_cast<uint64_t*>(
-      (reinterpret_cast<uintptr_t>(dn + N) + 7) & ~uintptr_t(7));
-  uint64_t* mbar = gk + 8;  // [2]
+  uint8_t* sB = sA + kFusedABytes;  // [2][hi|lo]
+  uint64_t* gp = reinterpret_cast<uint64_t*>(sB + 4 * bbytes);  // part index -> global offset
+  uint64_t* gn = gp + 64;                                        // column -> global offset
+  uint64_t* mbar = gn + N;                                       // [2]
   uint32_t* tmem_base = reinterpret_cast<uint32_t*>(mbar + 2);
 
   {
@@ -328,24 +331,23 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   uint32_t pmask = 0;
   for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[0][b];
   for (int p = t; p < 64; p += kK4Threads) {
-    uint32_t x = 0;
-    for (int b = 0; b < kFusedBits; ++b) x |= uint32_t((p >> b) & 1) << P.pbits[0][b];
-    dp[p] = uint16_t(tswz(x));
+    uint64_t x = 0;
+    for (int b = 0; b < kFusedBits; ++b) x |= uint64_t((p >> b) & 1) << P.pbits[0][b];
+    gp[p] = dep(x, P.tile);
   }
   for (int nn = t; nn < N; nn += kK4Threads) {
-    uint32_t x = 0, bit = 0;
+    uint64_t x = 0;
+    int bit = 0;
     for (int b = 0; b < m; ++b)
-      if (!((pmask >> b) & 1)) x |= uint32_t((nn >> bit++) & 1) << b;
-    dn[nn] = uint16_t(tswz(x));
+      if (!((pmask >> b) & 1)) x |= uint64_t((nn >> bit++) & 1) << b;
+    gn[nn] = dep(x, P.tile);
   }
-  const int chunks = T / 2, rows = chunks / kK4Threads;
-  for (int r = t; r < rows; r += kK4Threads) gk[r] = dep(uint64_t(r) * kK4Threads * 2, P.tile);
   if (t == 0) {
     tc::mbar_init(&mbar[0], 1);
     tc::mbar_init(&mbar[1], 1);
   }
   if (warp == 0) {
-    tc::tmem_alloc(tmem_base, 2 * kK4TmemCols);
+    tc::tmem_alloc(tmem_base, 2 * kK4DirectCols);
     tc::tmem_relinquish();
   }
   tc::fence_proxy_async_smem();
@@ -353,81 +355,43 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tmem_base;
-  const uint64_t gt = dep(uint64_t(t) * 2, P.tile);
   const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
   const int nprod = P.precision == 1 ? 1 : 3;
+  const int nitems = (N * 16) / kK4Threads;  // 2..8
+  const bool pairs = (gn[1] == 1);  // column bit 0 is global slot 0: columns pair up in 16 B
   uint32_t phase[2] = {0, 0};
-  bool pend[2] = {false, false};  // an MMA group committed to mbar[b] and not yet awaited
+  bool pend[2] = {false, false};
   bool failed = false;
-  auto xbuf = [&](int i) { return X0 + (i % 3) * 2 * T; };
-  auto issue_load = [&](uint64_t tl, float* dst) {
-    const uint64_t gb = dep(tl, P.outer);
-    const uint32_t ds = tc::smem_u32(dst);
-    for (int r = 0; r < rows; ++r)
-      cp_async16(ds + tswz(2u * uint32_t(t + r * kK4Threads)) * 8u, sv + gb + gt + gk[r]);
-  };
-  // tiles of this CTA: blockIdx.x + i * gridDim.x, i < cnt
   const uint64_t cnt =
       blockIdx.x < P.ntiles ? (P.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
   auto tile_of = [&](uint64_t i) { return blockIdx.x + i * gridDim.x; };
-  if (cnt > 0) issue_load(tile_of(0), xbuf(0));
-  cp_async_commit();
-  if (cnt > 1) issue_load(tile_of(1), xbuf(1));
-  cp_async_commit();
 
-  // drain tile j: TMEM accumulator j%2 -> X(j) -> global
-  auto drain = [&](uint64_t j) -> bool {
-    const int b = int(j & 1);
-    const bool ok = tc::mbar_wait(&mbar[b], phase[b], kWaitLimit);
-    if (__syncthreads_or(!ok)) return false;
-    phase[b] ^= 1u;
-    pend[b] = false;
-    tc::tc_fence_after();
-    float* X = xbuf(int(j % 3));
-    {
-      const int quad = warp & 3, half = warp >> 2;
-      const int r = quad * 32 + lane;
-      const int comp = r & 1;
-      const uint32_t prow = dp[r >> 1];
-      const int per_half = N / 2 < 16 ? 16 : N / 2;
-      const int c_begin = half * per_half;
-      const int c_end = c_begin + per_half < N ? c_begin + per_half : N;
-      for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
-        float d[16];
-        tc::tmem_ld16(tmem + uint32_t(b) * kK4TmemCols + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
-        const uint32_t* cw = reinterpret_cast<const uint32_t*>(dn + c0);
+  // this thread's B items: item = t + k * 256 -> (kb, nn)
+  float2 L[kK4DirectItems][4];
+  auto load_tile = [&](uint64_t i) {
+    const float2* base = sv + dep(tile_of(i), P.outer);
 #pragma unroll
-        for (int q = 0; q < 16; q += 2) {
-          const uint32_t w = cw[q >> 1];
-          X[2 * (prow ^ (w & 0xffffu)) + comp] = d[q];
-          X[2 * (prow ^ (w >> 16)) + comp] = d[q + 1];
-        }
-      }
+    for (int k = 0; k < kK4DirectItems; ++k) {
+      if (k >= nitems) break;
+      const int item = t + k * kK4Threads;
+      const int kb = item >> lgN, nn = item & (N - 1);
+      const float2* col = base + gn[nn];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) L[k][q] = __ldcs(col + gp[4 * kb + q]);
     }
-    tc::tc_fence_before();
-    __syncthreads();
-    const uint64_t gbase = dep(tile_of(j), P.outer);
-    for (int r = 0; r < rows; ++r) {
-      const uint4 v = *reinterpret_cast<const uint4*>(X + 2 * tswz(2u * uint32_t(t + r * kK4Threads)));
-      __stcs(reinterpret_cast<uint4*>(sv + gbase + gt + gk[r]), v);
-    }
-    __syncthreads();  // X(j) may be refilled
-    return true;
   };
-
-  for (uint64_t i = 0; i < cnt; ++i) {
-    cp_async_wait1();  // tile i has landed (tile i+1 may be in flight)
-    __syncthreads();
-    const float* X = xbuf(int(i % 3));
+  auto build_b = [&](uint64_t i) {
     uint8_t* bh = sB + (i & 1) * 2 * bbytes;
     uint8_t* bl = bh + bbytes;
-    for (int item = t; item < N * 16; item += kK4Threads) {
+#pragma unroll
+    for (int k = 0; k < kK4DirectItems; ++k) {
+      if (k >= nitems) break;
+      const int item = t + k * kK4Threads;
       const int kb = item >> lgN, nn = item & (N - 1);
-      const uint32_t col = dn[nn];
       uint32_t hw[4], lw[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float2 x = *reinterpret_cast<const float2*>(X + 2 * (dp[4 * kb + q] ^ col));
+        const float2 x = L[k][q];
         const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
         const float2 hf = __bfloat1622float2(h);
         const __nv_bfloat162 l = __floats2bfloat162_rn(x.x - hf.x, x.y - hf.y);
@@ -438,14 +402,61 @@ __global__ void __launch_bounds__(kK4Threads, 1)
       *reinterpret_cast<uint4*>(bh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
       *reinterpret_cast<uint4*>(bl + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
+  };
+  // TMEM accumulator of tile j -> global memory
+  auto drain = [&](uint64_t j) -> bool {
+    const int b = int(j & 1);
+    const bool ok = tc::mbar_wait(&mbar[b], phase[b], kWaitLimit);
+    if (__syncthreads_or(!ok)) return false;
+    phase[b] ^= 1u;
+    pend[b] = false;
+    tc::tc_fence_after();
+    const int quad = warp & 3, half = warp >> 2;
+    const int r = quad * 32 + lane;  // TMEM lane = D row = 2 p + c
+    const int comp = r & 1;
+    float2* base = sv + dep(tile_of(j), P.outer) + gp[r >> 1];
+    const int per_half = N / 2 < 16 ? 16 : N / 2;
+    const int c_begin = half * per_half;
+    const int c_end = c_begin + per_half < N ? c_begin + per_half : N;
+    for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
+      float d[16];
+      tc::tmem_ld16(tmem + uint32_t(b) * kK4DirectCols + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
+      // pair re / im with the neighbouring lane: the even lane keeps columns
+      // c0..c0+7, the odd lane c0+8..c0+15
+      float o[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) o[k] = __shfl_xor_sync(0xffffffffu, comp ? d[k] : d[8 + k], 1);
+      const int cb = c0 + (comp ? 8 : 0);
+      if (pairs) {
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+          const float4 v = comp ? make_float4(o[k], d[8 + k], o[k + 1], d[9 + k])
+                                : make_float4(d[k], o[k], d[k + 1], o[k + 1]);
+          __stcs(reinterpret_cast<float4*>(base + gn[cb + k]), v);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float2 v = comp ? make_float2(o[k], d[8 + k]) : make_float2(d[k], o[k]);
+          __stcs(base + gn[cb + k], v);
+        }
+      }
+    }
+    tc::tc_fence_before();
+    return true;
+  };
+
+  if (cnt > 0) load_tile(0);
+  for (uint64_t i = 0; i < cnt; ++i) {
+    build_b(i);  // B(i%2) was last read by the MMAs of tile i-2, drained before
     tc::fence_proxy_async_smem();
     tc::tc_fence_before();
     __syncthreads();
     if (t == 0) {
       tc::tc_fence_after();
       const uint32_t a0 = tc::smem_u32(sA);
-      const uint32_t bhs = tc::smem_u32(bh), bls = tc::smem_u32(bl);
-      const uint32_t d = tmem + uint32_t(i & 1) * kK4TmemCols;
+      const uint32_t bhs = tc::smem_u32(sB + (i & 1) * 2 * bbytes), bls = bhs + bbytes;
+      const uint32_t d = tmem + uint32_t(i & 1) * kK4DirectCols;
       uint32_t acc = 0;
       for (int prod = 0; prod < nprod; ++prod) {
         const uint32_t abase = a0 + (prod == 2 ? uint32_t(kFusedABytes / 2) : 0u);
@@ -460,25 +471,21 @@ __global__ void __launch_bounds__(kK4Threads, 1)
       tc::mma_commit(&mbar[i & 1]);
     }
     pend[i & 1] = true;
-    // while tile i multiplies: drain tile i-1, then refill its buffer with tile i+2
+    if (i + 1 < cnt) load_tile(i + 1);  // in flight while tile i multiplies and i-1 drains
     if (i > 0 && !drain(i - 1)) {
       failed = true;
       break;
     }
-    if (i + 2 < cnt) issue_load(tile_of(i + 2), xbuf(int((i + 2) % 3)));
-    cp_async_commit();
   }
   if (!failed && cnt > 0 && !drain(cnt - 1)) failed = true;
   if (failed) {
     if (t == 0) atomicExch(err, 1);
-    // the MMAs still in flight complete (or time out) before TMEM is freed
     for (int b = 0; b < 2; ++b)
       if (pend[b]) tc::mbar_wait(&mbar[b], phase[b], kWaitLimit);
   }
-  cp_async_wait0();
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4TmemCols);
+  if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4DirectCols);
 }
 
 }  // namespace
@@ -512,6 +519,24 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     attr = true;
   }
   const int T = 1 << P.m, N = T >> kFusedBits;
+  if (P.nops == 1) {
+    // direct form: A, two B buffers, offset tables, barriers
+    static bool dattr = false;
+    if (!dattr) {
+      HS_CUDA(cudaFuncSetAttribute(k4_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+      dattr = true;
+    }
+    const size_t dsmem = size_t(kFusedABytes) + size_t(N) * 1024 + 64 * 8 + size_t(N) * 8 + 16 + 16;
+    if (P.m > 13) return set_error(HS_E_UNSUPPORTED, "K4 tiles up to 2^13");
+    int dsms = 148, ddev = 0;
+    HS_CUDA(cudaGetDevice(&ddev));
+    HS_CUDA(cudaDeviceGetAttribute(&dsms, cudaDevAttrMultiProcessorCount, ddev));
+    const int dgrid = int(P.ntiles < uint64_t(dsms) ? P.ntiles : uint64_t(dsms));
+    k4_direct<<<dgrid, kK4Threads, dsmem, s>>>(static_cast<float2*>(amp), P,
+                                               static_cast<const uint8_t*>(d_a), d_err);
+    HS_CUDA(cudaGetLastError());
+    return HS_OK;
+  }
   // A operands, B hi/lo, two tile buffers, the dp/dn tables, chunk offsets
   // (8-byte aligned), mbarrier, TMEM address
   const size_t tables = (size_t(P.nops) * (64 + N) * 2 + 7) & ~size_t(7);
@@ -526,23 +551,6 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
   if (per_sm < 1) return set_error(HS_E_UNSUPPORTED, "K4 pass does not fit an SM");
   const uint64_t want = uint64_t(sms) * uint64_t(per_sm);
   const int grid = int(P.ntiles < want ? P.ntiles : want);
-  if (P.nops == 1) {
-    // pipelined form: A, two B buffers, three tile buffers, tables
-    static bool pattr = false;
-    if (!pattr) {
-      HS_CUDA(cudaFuncSetAttribute(k4_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-      pattr = true;
-    }
-    const size_t psmem = size_t(kFusedABytes) + size_t(N) * 1024 + size_t(T) * 24 +
-                         ((size_t(64 + N) * 2 + 7) & ~size_t(7)) + 8 * 8 + 16 + 16;
-    if (psmem <= 227 * 1024) {
-      const int pgrid = int(P.ntiles < uint64_t(sms) ? P.ntiles : uint64_t(sms));
-      k4_pipe<<<pgrid, kK4Threads, psmem, s>>>(static_cast<float2*>(amp), P,
-                                               static_cast<const uint8_t*>(d_a), d_err);
-      HS_CUDA(cudaGetLastError());
-      return HS_OK;
-    }
-  }
   k4_fused<<<grid, kK4Threads, smem, s>>>(static_cast<float2*>(amp), P,
                                           static_cast<const uint8_t*>(d_a), d_err);
   HS_CUDA(cudaGetLastError());

@@ -201,8 +201,9 @@ int hs_fused_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_o
  * gather_and_execute_on for a part whose unitary the caller already has. */
 int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int precision,
                    void* stream);
-/* Shape of the fused passes: unitaries applied per state pass (1..2) and
- * tile bits (10..12).  Returns the previous shape as ops * 100 + bits. */
+/* Shape of the fused passes: unitaries applied per state pass and tile bits,
+ * 1 with 10..13 (default 1, 13: operands straight from and to HBM) or 2 with
+ * 10..12.  Returns the previous shape as ops * 100 + bits. */
 int hs_set_fused_shape(int max_ops_per_pass, int tile_bits);
 int hs_fused_compose(int num_qubits, const hs_gate* gates, const int32_t* part_offsets,
                      int num_parts, double* out_u, int32_t* out_qubits);

@@ -105,10 +105,10 @@ def test_fused_errors():
         abi.State(12, abi.C64).run_fused(to_records(big), np.array([0, 7]))
 
 
-@pytest.mark.parametrize("shape", [(1, 10), (1, 11), (1, 12), (2, 11), (2, 12)])
+@pytest.mark.parametrize("shape", [(1, 10), (1, 11), (1, 12), (1, 13), (2, 11), (2, 12)])
 def test_fused_pass_shapes(port, shape):
-    """Every pass shape (unitaries per pass, tile bits) gives the same result;
-    (1, 11) runs two CTAs per SM."""
+    """Every pass shape (unitaries per pass, tile bits) gives the same result
+    (one unitary per pass: operands straight from and to HBM)."""
     n = 15
     gates = circuits.random_u3_cz(n, 8, 17)
     parts = partition.partition_acyclic(gates, 6)
