@@ -388,13 +388,20 @@ def main():
         fpasses = cf["passes"] / args.steps
         fbytes = 2.0 * (1 << n) * 8
         k4_ms = cf["apply_us"] / 1e3 / max(1, cf["passes"])
+        shape = abi.set_fused_shape(1, 13)
+        abi.set_fused_shape(shape // 100, shape % 100)
+        kname = "k4_direct" if shape // 100 == 1 else "k4_fused"
+        # tensor work: three BF16 products of a 128 x 128 real GEMM per amplitude column
+        tflops = 3 * 8.0 * 64 * (1 << n) * fpasses / t_f / 1e12
         fused = {"circuit_s": t_f, "parts": len(fparts), "passes_per_step": fpasses,
+                 "shape": {"unitaries_per_pass": shape // 100, "tile_bits": shape % 100},
                  "value": world * upd / t_f, "unit": UNIT,
                  "hbm_GBps": fpasses * fbytes / t_f / 1e9,
-                 "roofline": {"bound": "hbm", "kernel": "k4_fused", "avg_launch_ms": k4_ms,
+                 "roofline": {"bound": "hbm", "kernel": kname, "avg_launch_ms": k4_ms,
                               "achieved": fbytes / (k4_ms / 1e3) / 1e9 if k4_ms else None,
                               "peak": peak_gbs, "unit": "GB/s",
-                              "frac": fbytes / (k4_ms / 1e3) / 1e9 / peak_gbs if k4_ms else None},
+                              "frac": fbytes / (k4_ms / 1e3) / 1e9 / peak_gbs if k4_ms else None,
+                              "tensor_tflops": tflops},
                  "dtype": "c64 state, bf16x3 split operands, fp32 accumulate, fp64 unitaries",
                  "clocks": clk_f}
         if rank == 0 and not args.no_fidelity:

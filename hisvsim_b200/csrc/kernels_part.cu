@@ -242,23 +242,42 @@ __device__ __forceinline__ void op_xfer(const V (&s)[1 << R], V (&d)[1 << R], in
 #undef X2
 }
 
+// A per-thread sign that commutes with every op of a group: sign flips whose
+// mask lies wholly in thread / outer bits negate all of a thread's
+// amplitudes, so they are collected and applied once when the group ends.
+template <typename V>
+struct Deferred {
+  uint32_t sign = 0;  // 0 or the sign bit
+};
+
+template <int R, typename V>
+__device__ __forceinline__ void apply_deferred(V (&v)[1 << R], const Deferred<V>& d) {
+  constexpr int E = 1 << R;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    v[e].x = flip_sign(v[e].x, d.sign);
+    v[e].y = flip_sign(v[e].y, d.sign);
+  }
+}
+
 template <int R, bool FULL, typename V>
 __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, const double2* c,
-                                           uint32_t thr, uint64_t gbase) {
-  // thread and outer part of the controls; register part is in the code / creg
-  const bool ok = ((thr & op.cthr) == op.cthr) && ((gbase & op.couter) == op.couter);
-  const uint32_t sm = ok ? 0x80000000u : 0u;
-  const double2 f = ok ? c[0] : make_double2(1.0, 0.0);
+                                           uint32_t thr, uint64_t gbase, Deferred<V>& dfr) {
+  // thread and outer part of the controls (register part is in the code /
+  // creg); evaluated only by the ops that have such controls
+  auto ok = [&]() {
+    return ((thr & op.cthr) == op.cthr) && ((gbase & op.couter) == op.couter);
+  };
 #define C1(J) \
-  case 4 + (J): if constexpr ((J) < R) d1c<R, J>(v, c, op.creg, ok); break;
+  case 4 + (J): if constexpr ((J) < R) d1c<R, J>(v, c, op.creg, ok()); break;
 #define NEG(M) \
-  case 16 + (M): if constexpr ((M) < (1 << R)) dneg<R, M>(v, sm); break;
+  case 16 + (M): if constexpr ((M) < (1 << R)) dneg<R, M>(v, ok() ? 0x80000000u : 0u); break;
 #define PH(M) \
-  case 32 + (M): if constexpr ((M) < (1 << R)) dphase<R, M>(v, f); break;
+  case 32 + (M): if constexpr ((M) < (1 << R)) dphase<R, M>(v, ok() ? c[0] : make_double2(1.0, 0.0)); break;
 #define C2(P, JA, JB) \
-  case 72 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, op.creg, ok); break;
+  case 72 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, op.creg, ok()); break;
 #define SW(P, JA, JB) \
-  case 80 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, true>(v, c, op.creg, ok); break;
+  case 80 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, true>(v, c, op.creg, ok()); break;
 #define D1(J) \
   case (J): if constexpr ((J) < R) d1c<R, J>(v, c, 0u, true); break;
 #define D2(P, JA, JB) \
@@ -267,11 +286,14 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
     D1(0) D1(1) D1(2) D1(3)
     D2(0, 0, 1) D2(1, 0, 2) D2(2, 0, 3) D2(3, 1, 2) D2(4, 1, 3) D2(5, 2, 3)
     C1(0) C1(1) C1(2) C1(3)
-    NEG(0) NEG(1) NEG(2) NEG(3) NEG(4) NEG(5) NEG(6) NEG(7)
+    case 16:  // sign flip of every element of the thread (mask outside the registers)
+      dfr.sign ^= ok() ? 0x80000000u : 0u;
+      break;
+    NEG(1) NEG(2) NEG(3) NEG(4) NEG(5) NEG(6) NEG(7)
     NEG(8) NEG(9) NEG(10) NEG(11) NEG(12) NEG(13) NEG(14) NEG(15)
     PH(0) PH(1) PH(2) PH(3) PH(4) PH(5) PH(6) PH(7)
     PH(8) PH(9) PH(10) PH(11) PH(12) PH(13) PH(14) PH(15)
-    case 48: ddiag<R>(v, op, c, thr, gbase, ok); break;
+    case 48: ddiag<R>(v, op, c, thr, gbase, ok()); break;
     C2(0, 0, 1) C2(1, 0, 2) C2(2, 0, 3) C2(3, 1, 2) C2(4, 1, 3) C2(5, 2, 3)
     SW(0, 0, 1) SW(1, 0, 2) SW(2, 0, 3) SW(3, 1, 2) SW(4, 1, 3) SW(5, 2, 3)
     default: break;
@@ -402,6 +424,7 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
       // parameter space, so every dispatch below is a uniform branch
       int o = G.first_op;
       const int o_end = G.first_op + G.num_ops;
+      Deferred<V> dfr;
     in_v:
       while (o < o_end) {
         const DevOp& op = P.ops[o++];
@@ -409,8 +432,9 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
           op_xfer<R, FULL>(v, w, op.code, P.coef + op.coef);
           goto in_w;
         }
-        op_inplace<R, FULL>(v, op, P.coef + op.coef, thr, gbase);
+        op_inplace<R, FULL>(v, op, P.coef + op.coef, thr, gbase, dfr);
       }
+      apply_deferred<R>(v, dfr);
 #pragma unroll
       for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr(e)) = v[e];
       goto group_done;
@@ -421,8 +445,9 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
           op_xfer<R, FULL>(w, v, op.code, P.coef + op.coef);
           goto in_v;
         }
-        op_inplace<R, FULL>(w, op, P.coef + op.coef, thr, gbase);
+        op_inplace<R, FULL>(w, op, P.coef + op.coef, thr, gbase, dfr);
       }
+      apply_deferred<R>(w, dfr);
 #pragma unroll
       for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr(e)) = w[e];
     group_done:
