@@ -304,9 +304,10 @@ __global__ void __launch_bounds__(kK4Threads, 2)
 // amplitude of N = 64).  Tile i's MMAs run while tile i+1's loads are in flight
 // and tile i-1 drains; two TMEM accumulators and two B buffers alternate.
 // Shared memory: [A][B0 hi|lo][B1 hi|lo][gp: 64 x u64][gn: N x u64][2 mbarriers][TMEM address]
-constexpr int kK4DirectItems = 8;  // B items per thread (N * 16 / 256 for N = 128)
+constexpr int kK4DirectThreads = 512;  // 16 warps: four per TMEM lane quadrant
+constexpr int kK4DirectItems = 4;      // B items per thread (N * 16 / 512 for N = 128)
 
-__global__ void __launch_bounds__(kK4Threads, 1)
+__global__ void __launch_bounds__(kK4DirectThreads, 1)
     k4_direct(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
               const uint8_t* __restrict__ a_all, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t sm[];
@@ -326,16 +327,16 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   {
     const uint4* src = reinterpret_cast<const uint4*>(a_all + size_t(P.part[0]) * kFusedABytes);
     uint4* dst = reinterpret_cast<uint4*>(sA);
-    for (int i = t; i < kFusedABytes / 16; i += kK4Threads) dst[i] = src[i];
+    for (int i = t; i < kFusedABytes / 16; i += kK4DirectThreads) dst[i] = src[i];
   }
   uint32_t pmask = 0;
   for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[0][b];
-  for (int p = t; p < 64; p += kK4Threads) {
+  for (int p = t; p < 64; p += kK4DirectThreads) {
     uint64_t x = 0;
     for (int b = 0; b < kFusedBits; ++b) x |= uint64_t((p >> b) & 1) << P.pbits[0][b];
     gp[p] = dep(x, P.tile);
   }
-  for (int nn = t; nn < N; nn += kK4Threads) {
+  for (int nn = t; nn < N; nn += kK4DirectThreads) {
     uint64_t x = 0;
     int bit = 0;
     for (int b = 0; b < m; ++b)
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(kK4Threads, 1)
   const uint32_t tmem = *tmem_base;
   const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
   const int nprod = P.precision == 1 ? 1 : 3;
-  const int nitems = (N * 16) / kK4Threads;  // 2..8
+  const int nitems = (N * 16 + kK4DirectThreads - 1) / kK4DirectThreads;  // 1..4
   const bool pairs = (gn[1] == 1);  // column bit 0 is global slot 0: columns pair up in 16 B
   uint32_t phase[2] = {0, 0};
   bool pend[2] = {false, false};
@@ -373,7 +374,8 @@ __global__ void __launch_bounds__(kK4Threads, 1)
 #pragma unroll
     for (int k = 0; k < kK4DirectItems; ++k) {
       if (k >= nitems) break;
-      const int item = t + k * kK4Threads;
+      const int item = t + k * kK4DirectThreads;
+      if (item >= N * 16) break;
       const int kb = item >> lgN, nn = item & (N - 1);
       const float2* col = base + gn[nn];
 #pragma unroll
@@ -386,7 +388,8 @@ __global__ void __launch_bounds__(kK4Threads, 1)
 #pragma unroll
     for (int k = 0; k < kK4DirectItems; ++k) {
       if (k >= nitems) break;
-      const int item = t + k * kK4Threads;
+      const int item = t + k * kK4DirectThreads;
+      if (item >= N * 16) break;
       const int kb = item >> lgN, nn = item & (N - 1);
       uint32_t hw[4], lw[4];
 #pragma unroll
@@ -411,13 +414,15 @@ __global__ void __launch_bounds__(kK4Threads, 1)
     phase[b] ^= 1u;
     pend[b] = false;
     tc::tc_fence_after();
-    const int quad = warp & 3, half = warp >> 2;
+    // warp w reads TMEM lanes 32 (w % 4) ..; the four warps of a lane quadrant
+    // split the columns
+    const int quad = warp & 3, part_of_quad = warp >> 2;
     const int r = quad * 32 + lane;  // TMEM lane = D row = 2 p + c
     const int comp = r & 1;
     float2* base = sv + dep(tile_of(j), P.outer) + gp[r >> 1];
-    const int per_half = N / 2 < 16 ? 16 : N / 2;
-    const int c_begin = half * per_half;
-    const int c_end = c_begin + per_half < N ? c_begin + per_half : N;
+    const int per = N / 4 < 16 ? 16 : N / 4;
+    const int c_begin = part_of_quad * per;
+    const int c_end = c_begin + per < N ? c_begin + per : N;
     for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
       float d[16];
       tc::tmem_ld16(tmem + uint32_t(b) * kK4DirectCols + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
@@ -532,7 +537,7 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     HS_CUDA(cudaGetDevice(&ddev));
     HS_CUDA(cudaDeviceGetAttribute(&dsms, cudaDevAttrMultiProcessorCount, ddev));
     const int dgrid = int(P.ntiles < uint64_t(dsms) ? P.ntiles : uint64_t(dsms));
-    k4_direct<<<dgrid, kK4Threads, dsmem, s>>>(static_cast<float2*>(amp), P,
+    k4_direct<<<dgrid, kK4DirectThreads, dsmem, s>>>(static_cast<float2*>(amp), P,
                                                static_cast<const uint8_t*>(d_a), d_err);
     HS_CUDA(cudaGetLastError());
     return HS_OK;
