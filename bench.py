@@ -486,6 +486,27 @@ def main():
     fp64 = {"fma_per_step": fma_step, "achieved_tflops": 2 * fma_step / k1_total_s / 1e12,
             "peak_tflops": fp64_peak, "source": "hs_fp64_peak (measured FP64 FMA probe)",
             "frac": 2 * fma_step / k1_total_s / 1e12 / fp64_peak}
+    # K2: one in-place bit-swap pass over the same state (the redistribution
+    # kernel), timed by CUDA events; half the amplitudes move
+    k2 = None
+    try:
+        pairs = [(0, n - 1), (1, n - 2), (2, n - 3)]
+        st.permute_bits(pairs)
+        abi.synchronize()
+        a, b = abi.Event(), abi.Event()
+        a.record()
+        for _ in range(3):
+            st.permute_bits(pairs)
+        b.record()
+        abi.synchronize()
+        k2_ms = a.elapsed_ms(b) / 3
+        moved = (1 << n) * 16 * (1 - 0.5 ** len(pairs))  # amplitudes whose index changes
+        k2 = {"kernel": "k2_bitswap", "pairs": len(pairs), "avg_launch_ms": k2_ms,
+              "algorithmic_bytes_per_launch": 2 * moved,
+              "achieved_GBps": 2 * moved / (k2_ms / 1e3) / 1e9,
+              "frac": 2 * moved / (k2_ms / 1e3) / 1e9 / peak_gbs}
+    except Exception as ex:  # keep the headline if the extra measurement fails
+        k2 = {"error": str(ex)}
     st.close()
     del st
 
@@ -559,6 +580,7 @@ def main():
                          "kernel": "k1_part", "algorithmic_bytes_per_launch": bytes_per_pass,
                          "avg_launch_ms": k1_avg_ms, "fp64": fp64},
             "fused": fused,
+            "redistribution": k2,
             "batch": batch,
             "learned": learned_res,
             "gpu_launches": int(c["passes"] + args.steps),
