@@ -3,7 +3,9 @@
 Workload (seeded synthetic stand-in for the reference's QASMBench-style
 circuits): 40 layers of U3 with uniform angles on every qubit followed by CZ
 on a random matching (33 is odd: one qubit idles per layer), 1960 gates,
-state |0...0>, acyclic parts of <= k qubits from hisvsim_b200.partition.
+state |0...0>, acyclic parts of <= k qubits from hisvsim_b200.partition
+(consecutive runs of a DFS topological order by default; --partitioner
+acyclic selects the greedy acyclic partitioner).
 
 A step simulates the whole circuit once.  `value` is the plain complex128
 form's throughput in amplitude updates per second (sum over gates of 2^n,
@@ -43,6 +45,9 @@ def parse():
     ap.add_argument("--qubits", type=int, default=33)
     ap.add_argument("--layers", type=int, default=40)
     ap.add_argument("--part-qubits", type=int, default=9)
+    ap.add_argument("--partitioner", default="dfs", choices=["dfs", "acyclic"],
+                    help="acyclic parts from consecutive runs of a DFS topological order "
+                         "(default) or the greedy acyclic partitioner")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-qubits", type=int, default=26, help="size of the CPU sample")
     ap.add_argument("--cpu-layers", type=int, default=8)
@@ -152,12 +157,18 @@ class ClockSampler:
 
 # ---- workload ------------------------------------------------------------------
 
-def workload(n, layers, seed, k):
+def partitioner(args):
+    from hisvsim_b200 import partition
+
+    return partition.partition_dfs if args.partitioner == "dfs" else partition.partition_acyclic
+
+
+def workload(n, layers, seed, k, split=None):
     from hisvsim_b200 import circuits, partition
     from hisvsim_b200.gates import part_offsets
 
     gates = circuits.random_u3_cz(n, layers, seed)
-    parts = partition.partition_acyclic(gates, k)
+    parts = (split or partition.partition_acyclic)(gates, k)
     rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
     return gates, parts, rec, offs
 
@@ -225,8 +236,9 @@ def fidelity_small(args, abi, n):
     from hisvsim_b200 import partition
     from hisvsim_b200.gates import part_offsets
 
-    gates, parts, rec, offs = workload(n, args.layers, args.seed, args.part_qubits)
-    fparts = partition.partition_acyclic(gates, 6)
+    gates, parts, rec, offs = workload(n, args.layers, args.seed, args.part_qubits,
+                                       partitioner(args))
+    fparts = partitioner(args)(gates, 6)
     frec, foffs = part_offsets(partition.parts_to_gates(gates, fparts))
     a = abi.State(n, abi.C64)
     a.set_basis(0)
@@ -391,7 +403,8 @@ def main():
     if args.tile_qubits:
         abi.set_tile_qubits(args.tile_qubits)
     n = args.qubits
-    gates, parts, rec, offs = workload(n, args.layers, args.seed + rank, args.part_qubits)
+    gates, parts, rec, offs = workload(n, args.layers, args.seed + rank, args.part_qubits,
+                                       partitioner(args))
     upd = len(gates) * float(1 << n)
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -407,7 +420,7 @@ def main():
     if not args.no_fused:
         if args.fused_shape:
             abi.set_fused_shape(*[int(x) for x in args.fused_shape.split(",")])
-        fparts = partition.partition_acyclic(gates, 6)
+        fparts = partitioner(args)(gates, 6)
         frec, foffs = part_offsets(partition.parts_to_gates(gates, fparts))
         stf = abi.State(n, abi.C64)
 
@@ -569,7 +582,8 @@ def main():
             "config": {"workload": f"random circuit {n} qubits x {args.layers} layers "
                                    f"(U3 all qubits + CZ random matching), plain complex128",
                        "gates": len(gates), "parts": len(parts),
-                       "part_qubits": args.part_qubits, "tile_qubits": args.tile_qubits,
+                       "part_qubits": args.part_qubits, "partitioner": args.partitioner,
+                       "tile_qubits": args.tile_qubits,
                        "passes_per_step": passes, "state_bytes": (1 << n) * 16,
                        "l2": "state >> L2 (126 MB), no flush", "parallelism": f"replicas{world}"},
             "circuit_s": t_step, "hbm_GBps": passes * bytes_per_pass / t_step / 1e9,

@@ -321,27 +321,156 @@ int reduce_chunks(const void* amp, int dtype, int n, int chunk_bits, double* hos
   return HS_OK;
 }
 
+namespace {
+// Tiled form of K2: the tile holds every bit of the pass's pairs plus the
+// lowest other slots, so the permutation maps each tile onto itself.  A CTA
+// loads a tile (cp.async, double-buffered), then writes every element of it
+// back in global order, reading shared memory at the permuted position: one
+// coalesced read and one coalesced write of every amplitude.
+constexpr int kK2Threads = 256;
+constexpr int kK2MaxTileBits = 12;
+
+struct TilePerm {
+  Runs tile, outer;
+  int32_t m, np;
+  uint64_t ntiles;
+  uint8_t pa[8], pb[8];  // tile-bit positions of each pair
+};
+
+__device__ __forceinline__ uint64_t dep_runs(uint64_t x, const Runs& r) {
+  uint64_t out = 0;
+  for (int i = 0; i < r.n; ++i) out |= ((x >> r.src[i]) & ((1ull << r.len[i]) - 1ull)) << r.dst[i];
+  return out;
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async_el(uint32_t saddr, const void* g) {
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr), "l"(g) : "memory");
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kK2Threads) k2_tile(V* __restrict__ sv, const __grid_constant__ TilePerm P) {
+  extern __shared__ __align__(16) unsigned char smem_k2[];
+  const int t = threadIdx.x;
+  const int T = 1 << P.m;
+  const int per = T > kK2Threads ? T / kK2Threads : 1;
+  V* bufs = reinterpret_cast<V*>(smem_k2);
+  uint64_t* gk = reinterpret_cast<uint64_t*>(smem_k2 + 2 * size_t(T) * sizeof(V));
+  for (int k = t; k < per; k += kK2Threads) gk[k] = dep_runs(uint64_t(k) * kK2Threads, P.tile);
+  __syncthreads();
+  const bool active = t < T;
+  const uint64_t gt = dep_runs(uint64_t(t), P.tile);
+  const uint32_t sb = uint32_t(__cvta_generic_to_shared(bufs));
+  auto issue = [&](uint64_t tile, int b) {
+    if (!active) return;
+    const uint64_t gb = dep_runs(tile, P.outer) + gt;
+    for (int k = 0; k < per; ++k) {
+      const uint32_t j = uint32_t(t + k * kK2Threads);
+      cp_async_el<sizeof(V)>(sb + uint32_t((b * T + j) * sizeof(V)), sv + gb + gk[k]);
+    }
+  };
+  uint64_t tile = blockIdx.x;
+  if (tile < P.ntiles) issue(tile, 0);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (int it = 0; tile < P.ntiles; ++it, tile += gridDim.x) {
+    const uint64_t next = tile + gridDim.x;
+    if (next < P.ntiles) issue(next, (it + 1) & 1);
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 1;" ::: "memory");
+    __syncthreads();
+    const V* cur = bufs + (it & 1) * T;
+    if (active) {
+      const uint64_t gb = dep_runs(tile, P.outer) + gt;
+      for (int k = 0; k < per; ++k) {
+        uint32_t j = uint32_t(t + k * kK2Threads);
+        // element j receives the amplitude from the exchanged position
+        for (int i = 0; i < P.np; ++i) {
+          const uint32_t d = ((j >> P.pa[i]) ^ (j >> P.pb[i])) & 1u;
+          j ^= d * ((1u << P.pa[i]) | (1u << P.pb[i]));
+        }
+        __stcs(sv + gb + gk[k], cur[j]);
+      }
+    }
+    __syncthreads();  // this buffer is refilled by the prefetch issued next iteration
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+void runs_from(const std::vector<int>& dst, Runs* r) {
+  r->n = 0;
+  size_t i = 0;
+  while (i < dst.size()) {
+    size_t j = i + 1;
+    while (j < dst.size() && dst[j] == dst[j - 1] + 1) ++j;
+    r->src[r->n] = uint8_t(i);
+    r->len[r->n] = uint8_t(j - i);
+    r->dst[r->n] = uint8_t(dst[i]);
+    ++r->n;
+    i = j;
+  }
+}
+
+template <typename V>
+int launch_tile_perm(V* amp, int n, const int32_t* pairs, int np, int max_bits, cudaStream_t s) {
+  std::vector<int> tile;
+  for (int i = 0; i < np; ++i) {
+    tile.push_back(pairs[2 * i]);
+    tile.push_back(pairs[2 * i + 1]);
+  }
+  const int m = std::min(n, max_bits);
+  for (int sl = 0; sl < n && int(tile.size()) < m; ++sl)
+    if (std::find(tile.begin(), tile.end(), sl) == tile.end()) tile.push_back(sl);
+  std::sort(tile.begin(), tile.end());
+  TilePerm P{};
+  P.m = int(tile.size());
+  P.np = np;
+  P.ntiles = 1ull << (n - P.m);
+  runs_from(tile, &P.tile);
+  std::vector<int> outer;
+  for (int sl = 0; sl < n; ++sl)
+    if (std::find(tile.begin(), tile.end(), sl) == tile.end()) outer.push_back(sl);
+  runs_from(outer, &P.outer);
+  if (P.tile.n > kMaxRuns || P.outer.n > kMaxRuns)
+    return set_error(HS_E_UNSUPPORTED, "bit-swap tile has too many runs");
+  for (int i = 0; i < np; ++i) {
+    P.pa[i] = uint8_t(std::find(tile.begin(), tile.end(), pairs[2 * i]) - tile.begin());
+    P.pb[i] = uint8_t(std::find(tile.begin(), tile.end(), pairs[2 * i + 1]) - tile.begin());
+  }
+  const int T = 1 << P.m;
+  const int per = T > kK2Threads ? T / kK2Threads : 1;
+  const size_t smem = 2 * size_t(T) * sizeof(V) + size_t(per) * 8;
+  static bool attr = false;
+  if (!attr) {
+    HS_CUDA(cudaFuncSetAttribute(k2_tile<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr = true;
+  }
+  int per_sm = 1;
+  HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_tile<V>, kK2Threads, smem));
+  const uint64_t want = uint64_t(num_sms()) * uint64_t(std::max(per_sm, 1));
+  const int grid = int(P.ntiles < want ? P.ntiles : want);
+  k2_tile<V><<<grid, kK2Threads, smem, s>>>(amp, P);
+  HS_CUDA(cudaGetLastError());
+  return HS_OK;
+}
+}  // namespace
+
 int launch_permute(void* amp, int dtype, int n, const int32_t* pairs, int npairs,
                    cudaStream_t s) {
   if (npairs <= 0) return HS_OK;
   if (npairs > 32) return set_error(HS_E_INVALID, "at most 32 bit pairs per pass");
-  SwapPairs sp{};
-  sp.np = npairs;
-  for (int i = 0; i < npairs; ++i) {
-    sp.a[i] = uint8_t(pairs[2 * i]);
-    sp.b[i] = uint8_t(pairs[2 * i + 1]);
-    sp.ma |= 1ull << sp.a[i];
-    sp.mb |= 1ull << sp.b[i];
+  // pairs commute (they are disjoint): apply them in tiled passes of at most
+  // five pairs, each tile keeping at least one more low slot for contiguity
+  const int max_bits = dtype == HS_DTYPE_C128 ? 11 : kK2MaxTileBits;
+  const int chunk = std::min(5, std::max(1, (std::min(n, max_bits) - 1) / 2));
+  for (int first = 0; first < npairs; first += chunk) {
+    const int np = std::min(chunk, npairs - first);
+    if (dtype == HS_DTYPE_C128)
+      HS_TRY(launch_tile_perm(static_cast<double2*>(amp), n, pairs + 2 * first, np, max_bits, s));
+    else
+      HS_TRY(launch_tile_perm(static_cast<float2*>(amp), n, pairs + 2 * first, np, max_bits, s));
   }
-  const uint64_t size = 1ull << n;
-  const int threads = 256;
-  if (dtype == HS_DTYPE_C128)
-    k2_bitswap<double2><<<grid_for(size, threads), threads, 0, s>>>(static_cast<double2*>(amp),
-                                                                     size, sp);
-  else
-    k2_bitswap<float2><<<grid_for(size, threads), threads, 0, s>>>(static_cast<float2*>(amp),
-                                                                    size, sp);
-  HS_CUDA(cudaGetLastError());
   return HS_OK;
 }
 

@@ -25,16 +25,28 @@ def swapbits(x, pairs):
 
 
 @pytest.mark.parametrize("pairs", [[(0, 1)], [(0, 13)], [(2, 9), (4, 11)], [(12, 13)],
-                                   [(0, 7), (1, 8), (2, 9), (3, 10), (4, 11)]])
-def test_permute_bits(pairs):
+                                   [(0, 7), (1, 8), (2, 9), (3, 10), (4, 11)],
+                                   [(0, 13), (1, 12), (2, 11), (3, 10), (4, 9), (5, 8), (6, 7)]])
+@pytest.mark.parametrize("dtype", [abi.C128, abi.C64])
+def test_permute_bits(pairs, dtype):
     n = 14
-    st = prepared(n)
+    st = abi.State(n, dtype)
+    st.run_part(circuits.random_layered(n, 3, 3))
     base = st.raw()
     st.permute_bits([v for p in pairs for v in p])
     x = np.arange(1 << n)
     assert np.array_equal(st.raw()[swapbits(x, pairs)], base[x])
     st.canonicalize()
     assert np.array_equal(st.raw(), base)
+
+
+@pytest.mark.parametrize("n,pairs", [(3, [(0, 2)]), (5, [(0, 4), (1, 3)]), (22, [(0, 21), (3, 17)])])
+def test_permute_small_and_large_states(n, pairs):
+    st = prepared(n)
+    base = st.raw()
+    st.permute_bits([v for p in pairs for v in p])
+    x = np.arange(1 << n)
+    assert np.array_equal(st.raw()[swapbits(x, pairs)], base[x])
 
 
 @pytest.mark.parametrize("proc", [[0], [13], [2, 5, 7], [0, 1, 2, 3], [9, 3, 11, 6, 1]])
