@@ -94,6 +94,7 @@ SIGNATURES = {
     "hs_project": [_vp, _vp, _vp, _i, _i, ctypes.POINTER(_vp), _dp, _vp],
     "hs_fp64_peak": [_dp],
     "hs_set_fused_shape": [_i, _i],
+    "hs_set_k4_variant": [_i],
     "hs_fused_apply": [_vp, _vp, _vp, _i, _vp],
     "hs_permute_bits": [_vp, _vp, _i, _vp],
     "hs_gather_qubits": [_vp, _vp, _i, _vp],
@@ -548,6 +549,13 @@ class QaoaBatch:
 
 def set_fused_shape(max_ops_per_pass: int, tile_bits: int) -> int:
     r = lib().hs_set_fused_shape(max_ops_per_pass, tile_bits)
+    if r < 0:
+        check(r)
+    return r
+
+
+def set_k4_variant(variant: int) -> int:
+    r = lib().hs_set_k4_variant(variant)
     if r < 0:
         check(r)
     return r

@@ -249,6 +249,11 @@ int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int pre
   return HS_OK;
 }
 
+int hs_set_k4_variant(int variant) {
+  if (variant < 0 || variant > 1) return set_error(HS_E_INVALID, "K4 variant 0 or 1");
+  return set_k4_variant(variant);
+}
+
 int hs_set_fused_shape(int max_ops_per_pass, int tile_bits) {
   if (max_ops_per_pass < 1 || max_ops_per_pass > kFusedMaxOps || tile_bits < 10 ||
       tile_bits > (max_ops_per_pass == 1 ? 13 : 12))

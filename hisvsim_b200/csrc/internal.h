@@ -172,6 +172,7 @@ int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, 
 int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cudaStream_t s);
 // row-major 64 x 64 unitaries (nparts of them) -> A operands (real form, BF16 hi/lo)
 int launch_pack(const double2* d_u, int nparts, void* d_a, cudaStream_t s);
+int set_k4_variant(int v);  // one unitary per pass: 0 direct, 1 warp-specialised
 int reduce_compare(const void* a, int adtype, const void* b, int bdtype, int n, double out[4],
                    cudaStream_t s);
 int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, uint64_t count,

@@ -11,6 +11,8 @@
 // Ah*Bh + Ah*Bl + Al*Bh (the Al*Bl term, ~2^-16 relative, is dropped).
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "internal.h"
 #include "tcgen05.cuh"
 
@@ -493,7 +495,224 @@ __global__ void __launch_bounds__(kK4DirectThreads, 1)
   if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4DirectCols);
 }
 
+// ---- K4, one unitary per pass, warp-specialised ---------------------------------
+// Three roles run concurrently on one CTA per SM, handing tiles over through
+// mbarriers instead of CTA-wide barriers:
+//   warps 0-7   producers: load tile i from HBM into registers, split into
+//               BF16 hi / lo, write B(i%2), arrive on bfull(i%2);
+//   warp 16     one thread issues tile i's MMAs into TMEM accumulator i%2
+//               and commits them to mdone(i%2);
+//   warps 8-15  epilogue: wait mdone(i%2), move the accumulator from TMEM to
+//               HBM, arrive on tfree(i%2).
+// B(b) is rewritten only after mdone(b) of the tile two back, and
+// accumulator b only after tfree(b) of the tile two back, so loads, MMAs and
+// stores of three consecutive tiles overlap.  Every wait is bounded; a
+// timeout sets the error flag and the shared abort word, and the other roles
+// leave at their next wait.
+constexpr int kWsProducers = 256;
+constexpr int kWsThreads = 544;  // 8 producer warps, 8 epilogue warps, 1 MMA warp
+constexpr int kWsItems = 8;      // B items per producer thread (N * 16 / 256, N <= 128)
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
+}
+
+__global__ void __launch_bounds__(kWsThreads, 1)
+    k4_ws(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
+          const uint8_t* __restrict__ a_all, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m = P.m;
+  const int N = 1 << (m - kFusedBits);
+  const int lgN = m - kFusedBits;
+  const uint32_t bk = uint32_t(N) * 16u;
+  const uint32_t bbytes = uint32_t(N) * 256u;
+  uint8_t* sA = sm;
+  uint8_t* sB = sA + kFusedABytes;  // [2][hi|lo]
+  uint64_t* gp = reinterpret_cast<uint64_t*>(sB + 4 * bbytes);
+  uint64_t* gn = gp + 64;
+  uint64_t* bfull = gn + N;   // [2]
+  uint64_t* mdone = bfull + 2;  // [2]
+  uint64_t* tfree = mdone + 2;  // [2]
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tfree + 2);
+  uint32_t* tmem_base = reinterpret_cast<uint32_t*>(tfree + 3);
+
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a_all + size_t(P.part[0]) * kFusedABytes);
+    uint4* dst = reinterpret_cast<uint4*>(sA);
+    for (int i = t; i < kFusedABytes / 16; i += kWsThreads) dst[i] = src[i];
+  }
+  uint32_t pmask = 0;
+  for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[0][b];
+  for (int p = t; p < 64; p += kWsThreads) {
+    uint64_t x = 0;
+    for (int b = 0; b < kFusedBits; ++b) x |= uint64_t((p >> b) & 1) << P.pbits[0][b];
+    gp[p] = dep(x, P.tile);
+  }
+  for (int nn = t; nn < N; nn += kWsThreads) {
+    uint64_t x = 0;
+    int bit = 0;
+    for (int b = 0; b < m; ++b)
+      if (!((pmask >> b) & 1)) x |= uint64_t((nn >> bit++) & 1) << b;
+    gn[nn] = dep(x, P.tile);
+  }
+  if (t == 0) {
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&bfull[b], kWsProducers);
+      tc::mbar_init(&mdone[b], 1);
+      tc::mbar_init(&tfree[b], kWsProducers);  // the epilogue has as many threads
+    }
+    *abort_flag = 0;
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_base, 2 * kK4DirectCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_base;
+  const uint64_t cnt =
+      blockIdx.x < P.ntiles ? (P.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto tile_of = [&](uint64_t i) { return blockIdx.x + i * gridDim.x; };
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicExch(err, 1);
+  };
+
+  if (warp < 8) {
+    // ---- producers
+    const int nitems = (N * 16) / kWsProducers;  // 1..8
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i & 1);
+      float2 L[kWsItems][4];
+      const float2* base = sv + dep(tile_of(i), P.outer);
+#pragma unroll
+      for (int k = 0; k < kWsItems; ++k) {
+        if (k >= nitems) break;
+        const int item = t + k * kWsProducers;
+        const int kb = item >> lgN, nn = item & (N - 1);
+        const float2* col = base + gn[nn];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) L[k][q] = __ldcs(col + gp[4 * kb + q]);
+      }
+      if (i >= 2 && !tc::mbar_wait(&mdone[b], uint32_t((i - 2) >> 1) & 1u, kWaitLimit)) {
+        fail();
+        break;
+      }
+      uint8_t* bh = sB + b * 2 * bbytes;
+      uint8_t* bl = bh + bbytes;
+#pragma unroll
+      for (int k = 0; k < kWsItems; ++k) {
+        if (k >= nitems) break;
+        const int item = t + k * kWsProducers;
+        const int kb = item >> lgN, nn = item & (N - 1);
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 x = L[k][q];
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(x.x - hf.x, x.y - hf.y);
+          hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+          lw[q] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+        const uint32_t off = tc::kmajor_off(uint32_t(nn), uint32_t(kb * 8), bk);
+        *reinterpret_cast<uint4*>(bh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(bl + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+      }
+      tc::fence_proxy_async_smem();  // the B writes become visible to the tensor cores
+      mbar_arrive(&bfull[b]);
+    }
+  } else if (warp < 16) {
+    // ---- epilogue: TMEM accumulator -> HBM
+    const int quad = warp & 3, half = (warp - 8) >> 2;
+    const int r = quad * 32 + lane;
+    const int comp = r & 1;
+    const bool pairs = (gn[1] == 1);
+    const int per = N / 2 < 16 ? 16 : N / 2;
+    const int c_begin = half * per;
+    const int c_end = c_begin + per < N ? c_begin + per : N;
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i & 1);
+      if (!tc::mbar_wait(&mdone[b], uint32_t(i >> 1) & 1u, kWaitLimit)) {
+        fail();
+        break;
+      }
+      tc::tc_fence_after();
+      float2* base = sv + dep(tile_of(i), P.outer) + gp[r >> 1];
+      for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
+        float d[16];
+        tc::tmem_ld16(tmem + uint32_t(b) * kK4DirectCols + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
+        float o[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) o[k] = __shfl_xor_sync(0xffffffffu, comp ? d[k] : d[8 + k], 1);
+        const int cb = c0 + (comp ? 8 : 0);
+        if (pairs) {
+#pragma unroll
+          for (int k = 0; k < 8; k += 2) {
+            const float4 v = comp ? make_float4(o[k], d[8 + k], o[k + 1], d[9 + k])
+                                  : make_float4(d[k], o[k], d[k + 1], o[k + 1]);
+            __stcs(reinterpret_cast<float4*>(base + gn[cb + k]), v);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const float2 v = comp ? make_float2(o[k], d[8 + k]) : make_float2(d[k], o[k]);
+            __stcs(base + gn[cb + k], v);
+          }
+        }
+      }
+      tc::tc_fence_before();
+      mbar_arrive(&tfree[b]);
+    }
+  } else if (lane == 0) {
+    // ---- MMA issue
+    const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
+    const int nprod = P.precision == 1 ? 1 : 3;
+    const uint32_t a0 = tc::smem_u32(sA);
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i & 1);
+      if (!tc::mbar_wait(&bfull[b], uint32_t(i >> 1) & 1u, kWaitLimit) ||
+          (i >= 2 && !tc::mbar_wait(&tfree[b], uint32_t((i - 2) >> 1) & 1u, kWaitLimit))) {
+        fail();
+        break;
+      }
+      tc::tc_fence_after();
+      const uint32_t bhs = tc::smem_u32(sB + b * 2 * bbytes), bls = bhs + bbytes;
+      const uint32_t d = tmem + uint32_t(b) * kK4DirectCols;
+      uint32_t acc = 0;
+      for (int prod = 0; prod < nprod; ++prod) {
+        const uint32_t abase = a0 + (prod == 2 ? uint32_t(kFusedABytes / 2) : 0u);
+        const uint32_t bbase = prod == 1 ? bls : bhs;
+        for (int s = 0; s < 8; ++s) {
+          const uint64_t ad = tc::smem_desc(abase + uint32_t(s) * 2u * 2048u, 2048u, 128u);
+          const uint64_t bd = tc::smem_desc(bbase + uint32_t(s) * 2u * bk, bk, 128u);
+          tc::mma_bf16(d, ad, bd, idesc, acc);
+          acc = 1;
+        }
+      }
+      tc::mma_commit(&mdone[b]);
+      issued = i + 1;
+    }
+    // the last committed MMAs complete before TMEM is released
+    if (issued > 0) {
+      const uint64_t j = issued - 1;
+      tc::mbar_wait(&mdone[j & 1], uint32_t(j >> 1) & 1u, kWaitLimit);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4DirectCols);
+}
+
 }  // namespace
+
+std::atomic<int> g_k4_variant{1};  // one unitary per pass: 0 direct, 1 warp-specialised
+
+int set_k4_variant(int v) { return g_k4_variant.exchange(v); }
 
 int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, double2* d_u,
                    void* d_a, cudaStream_t s) {
@@ -524,6 +743,25 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     attr = true;
   }
   const int T = 1 << P.m, N = T >> kFusedBits;
+  if (P.nops == 1 && g_k4_variant.load() == 1) {
+    // warp-specialised form: A, two B buffers, offset tables, six mbarriers
+    static bool wattr = false;
+    if (!wattr) {
+      HS_CUDA(cudaFuncSetAttribute(k4_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+      wattr = true;
+    }
+    if (P.m > 13) return set_error(HS_E_UNSUPPORTED, "K4 tiles up to 2^13");
+    const size_t wsmem = size_t(kFusedABytes) + size_t(N) * 1024 + 64 * 8 + size_t(N) * 8 +
+                         6 * 8 + 8 + 16;
+    int wsms = 148, wdev = 0;
+    HS_CUDA(cudaGetDevice(&wdev));
+    HS_CUDA(cudaDeviceGetAttribute(&wsms, cudaDevAttrMultiProcessorCount, wdev));
+    const int wgrid = int(P.ntiles < uint64_t(wsms) ? P.ntiles : uint64_t(wsms));
+    k4_ws<<<wgrid, kWsThreads, wsmem, s>>>(static_cast<float2*>(amp), P,
+                                           static_cast<const uint8_t*>(d_a), d_err);
+    HS_CUDA(cudaGetLastError());
+    return HS_OK;
+  }
   if (P.nops == 1) {
     // direct form: A, two B buffers, offset tables, barriers
     static bool dattr = false;

@@ -18,10 +18,18 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                : "memory");
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Wait for the phase with the given parity to complete; gives up after
-// `limit` polls and returns false (the caller records a timeout).
+// `limit` polls or two seconds, whichever comes first, and returns false (the
+// caller records a timeout).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
   const uint32_t a = smem_u32(bar);
+  const uint64_t t0 = global_ns();
   for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
@@ -32,6 +40,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 63) == 63 && global_ns() - t0 > 2000000000ull) return false;
   }
   return false;
 }

@@ -148,3 +148,23 @@ def test_fused_apply_given_unitary():
     want = np.moveaxis(out, range(6), axes).reshape(-1)
     assert 1 - fid(want, got) <= 1e-8
     assert np.abs(got - want).max() <= 1e-5
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("n", [10, 13, 17])
+def test_k4_variants(port, variant, n):
+    """Both one-unitary-per-pass kernels (direct, warp-specialised) agree with
+    the oracle, including states with fewer tiles than SMs."""
+    gates = circuits.random_u3_cz(n, 6, 23)
+    parts = partition.partition_dfs(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    prev = abi.set_k4_variant(variant)
+    try:
+        st = abi.State(n, abi.C64)
+        st.run_fused(rec, offs, 0)
+        got = st.amplitudes().astype(complex)
+    finally:
+        abi.set_k4_variant(prev)
+    assert 1 - fid(want, got) <= 1e-8
+    assert np.abs(got - want).max() <= 1e-5
