@@ -44,9 +44,10 @@ __device__ __forceinline__ void cp_wait() {
 }
 
 struct Shared {
+  alignas(16) uint8_t cut[kTileMax];
+  BatchPass pass;  // the item's pass, copied once per item
   float2 phase[kBatchMaxEdges + 1];
   uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
-  uint8_t cut[kTileMax];
   uint64_t gk[kTileMax / 2 / kBatchThreads];  // global offset of chunk k*threads
   int w[16];
   int c;
@@ -125,7 +126,15 @@ __global__ void __launch_bounds__(kBatchThreads, 6)
     const BatchInstance& I = insts[G.inst];
     const int k = G.step;
     const int round = k / I.npasses, pj = k - round * I.npasses;
-    const BatchPass& P = I.pass[pj];
+    {
+      // the pass descriptor is read many times per tile: keep it in shared memory
+      static_assert(sizeof(BatchPass) % 4 == 0, "BatchPass words");
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&I.pass[pj]);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&S.pass);
+      for (int w = t; w < int(sizeof(BatchPass) / 4); w += kBatchThreads) dst[w] = src[w];
+    }
+    __syncthreads();
+    const BatchPass& P = S.pass;
     const int m = P.m, T = 1 << m, ngr = P.ngroups, nedges = I.nedges;
     const bool phase = P.phase != 0;
     const uint32_t t_begin = uint32_t(item - G.first) * G.chunk;
@@ -137,7 +146,9 @@ __global__ void __launch_bounds__(kBatchThreads, 6)
         S.ea[t] = I.edge_a[t];
         S.eb[t] = I.edge_b[t];
       }
-      for (int i = t; i < T; i += kBatchThreads) S.cut[i] = I.cut_low[i];
+      const uint4* cs = reinterpret_cast<const uint4*>(I.cut_low);
+      uint4* cd = reinterpret_cast<uint4*>(S.cut);
+      for (int i = t; i < T / 16; i += kBatchThreads) cd[i] = cs[i];
     }
     const float2 rx = pars[G.inst].rx[round][0];  // (cos beta, sin beta)
     const bool active = t < (T >> 4);
