@@ -83,6 +83,10 @@ __device__ __forceinline__ uint32_t swz(uint32_t i) {
 // specialized by their register mask so only the affected elements are
 // touched.
 
+__host__ __device__ constexpr int lowest_bit(int e) {
+  return (e & 1) ? 0 : (e & 2) ? 1 : (e & 4) ? 2 : (e & 8) ? 3 : (e & 16) ? 4 : 5;
+}
+
 template <int J>
 __device__ __forceinline__ constexpr int ins0(int p) {  // insert a 0 bit at J
   return ((p >> J) << (J + 1)) | (p & ((1 << J) - 1));
@@ -247,12 +251,14 @@ __device__ __forceinline__ void op_xfer(const V (&s)[1 << R], V (&d)[1 << R], in
 // amplitudes, so they are collected and applied once when the group ends.
 template <typename V>
 struct Deferred {
-  uint32_t sign = 0;  // 0 or the sign bit
+  uint32_t sign = 0;   // 0 or the sign bit
+  bool any = false;    // warp-uniform: a sign was deferred in this group
 };
 
 template <int R, typename V>
 __device__ __forceinline__ void apply_deferred(V (&v)[1 << R], const Deferred<V>& d) {
   constexpr int E = 1 << R;
+  if (!d.any) return;
 #pragma unroll
   for (int e = 0; e < E; ++e) {
     v[e].x = flip_sign(v[e].x, d.sign);
@@ -288,6 +294,7 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
     C1(0) C1(1) C1(2) C1(3)
     case 16:  // sign flip of every element of the thread (mask outside the registers)
       dfr.sign ^= ok() ? 0x80000000u : 0u;
+      dfr.any = true;
       break;
     NEG(1) NEG(2) NEG(3) NEG(4) NEG(5) NEG(6) NEG(7)
     NEG(8) NEG(9) NEG(10) NEG(11) NEG(12) NEG(13) NEG(14) NEG(15)
@@ -403,23 +410,28 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
       const uint32_t thr = uint32_t(deposit(t, G.thr));
-      uint32_t sx[R], lo[R];  // per register bit: swizzled slot part / in-slot part
+      // per register bit: the offset change of setting that bit (swizzled slot
+      // part and in-slot part occupy disjoint bits, so they combine by XOR and
+      // so do the bits of an element index)
+      uint32_t dx[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const uint32_t b = 1u << G.reg_tbit[j];
-        sx[j] = swz(b >> M::SH) << 4;
-        lo[j] = (b & ((1u << M::SH) - 1u)) * uint32_t(sizeof(V));
+        dx[j] = (swz(b >> M::SH) << 4) ^ ((b & ((1u << M::SH) - 1u)) * uint32_t(sizeof(V)));
       }
       const uint32_t sthr = M::off(thr);
-      auto addr = [&](int e) -> uint32_t {
-        uint32_t a = sthr;
+      // offsets of the E elements, each one XOR from an earlier one
+      auto offsets = [&](uint32_t (&a)[E]) {
+        a[0] = sthr;
 #pragma unroll
-        for (int j = 0; j < R; ++j)
-          if ((e >> j) & 1) a = (a ^ sx[j]) + lo[j];
-        return a;
+        for (int e = 1; e < E; ++e) a[e] = a[e & (e - 1)] ^ dx[lowest_bit(e)];
       };
+      {
+        uint32_t a[E];
+        offsets(a);
 #pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(A + addr(e));
+        for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(A + a[e]);
+      }
       // op descriptors and coefficients are read from the (warp-uniform)
       // parameter space, so every dispatch below is a uniform branch
       int o = G.first_op;
@@ -435,8 +447,12 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
         op_inplace<R, FULL>(v, op, P.coef + op.coef, thr, gbase, dfr);
       }
       apply_deferred<R>(v, dfr);
+      {
+        uint32_t a[E];
+        offsets(a);
 #pragma unroll
-      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr(e)) = v[e];
+        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + a[e]) = v[e];
+      }
       goto group_done;
     in_w:
       while (o < o_end) {
@@ -448,8 +464,12 @@ __global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
         op_inplace<R, FULL>(w, op, P.coef + op.coef, thr, gbase, dfr);
       }
       apply_deferred<R>(w, dfr);
+      {
+        uint32_t a[E];
+        offsets(a);
 #pragma unroll
-      for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + addr(e)) = w[e];
+        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + a[e]) = w[e];
+      }
     group_done:
       __syncthreads();  // the group's writes precede the next group's reads
     }
