@@ -309,6 +309,7 @@ def batch_form(args, abi, peak_gbs, pg, device):
             "bytes_per_run": st["bytes_per_run"], "work_items": st["items"],
             "tuned": {"tile_cap": cap, "ctas_per_sm": ctas, "best_ms": tune_ms,
                       "tiles_per_item": st["tiles_per_item"], "low_keep": st["low_keep"],
+                      "threads_per_cta": st["threads"], "ctas_per_sm_used": st["ctas_per_sm"],
                       "caps_by_qubits": {int(n): int(c) for n, c in zip(ns, caps)}},
             "max_hc_err_per_edge": worst, "checked_instances": check,
             "plain_c128_sequential_s": t_plain,

@@ -520,10 +520,10 @@ class QaoaBatch:
         return out, ms.value
 
     def stats(self):
-        s = np.zeros(7, dtype=np.int64)
+        s = np.zeros(8, dtype=np.int64)
         check(lib().hs_batch_stats(self.h, _ptr(s)))
         return dict(zip(["items", "steps", "bytes_per_run", "tile_cap", "ctas_per_sm",
-                         "tiles_per_item", "low_keep"], s.tolist()))
+                         "tiles_per_item", "low_keep", "threads"], s.tolist()))
 
     def tile_caps(self) -> np.ndarray:
         caps = np.zeros(self.count, dtype=np.int32)

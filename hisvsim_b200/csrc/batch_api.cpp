@@ -15,7 +15,8 @@ struct hs_batch {
   std::vector<int> n;
   std::vector<std::vector<std::pair<int, int>>> edges;
   std::vector<double> gammas, betas;
-  int tile_cap = kBatchMaxTileBits, ctas_per_sm = 6, chunk = 8;
+  int tile_cap = 11, ctas_per_sm = 16, chunk = 8;
+  int threads = 128;  // CTA size of the plan: 256 once some tile has 2^12 amplitudes
   int low_keep = 3;  // lowest qubits kept in every later pass's tile (contiguous runs)
   int cap_of_n[kBatchMaxQubits + 1] = {};  // per qubit count; 0 = tile_cap
   void* pool = nullptr;
@@ -177,6 +178,7 @@ int build_plan(hs_batch* b) {
   b->pass_bytes = 0;
   std::vector<size_t> cut_off(b->ninst);
   size_t cut_bytes = 0;
+  int max_m = 0;
   for (int i = 0; i < b->ninst; ++i) {
     BatchInstance& I = inst[i];
     I.amp = static_cast<float2*>(b->pool) + b->offset[i];
@@ -188,6 +190,7 @@ int build_plan(hs_batch* b) {
       I.edge_b[e] = uint8_t(b->edges[i][e].second);
     }
     HS_TRY(plan_passes(I.n, b->cap_of_n[I.n] ? b->cap_of_n[I.n] : b->tile_cap, b->low_keep, &I));
+    for (int j = 0; j < I.npasses; ++j) max_m = std::max(max_m, int(I.pass[j].m));
     I.step_base = nc;
     const int steps = I.npasses * b->p;
     nc += uint64_t(steps);
@@ -196,6 +199,7 @@ int build_plan(hs_batch* b) {
     cut_off[i] = cut_bytes;
     cut_bytes += size_t(1) << I.pass[0].m;
   }
+  b->threads = max_m > 11 ? 256 : 128;
   std::vector<uint8_t> cut(cut_bytes);
   for (int i = 0; i < b->ninst; ++i)
     cut_low_table(b->edges[i], inst[i].pass[0].m, cut.data() + cut_off[i]);
@@ -246,7 +250,8 @@ int build_plan(hs_batch* b) {
   if (rc == HS_OK)
     rc = launch_batch(b->d_inst, b->d_par, b->d_items, b->ngroups, b->total, b->d_counters,
                       b->d_head, b->d_err,
-                      sms * std::min(b->ctas_per_sm, batch_max_ctas_per_sm()), b->stream);
+                      sms * std::min(b->ctas_per_sm, batch_max_ctas_per_sm(b->threads)),
+                      b->threads, b->stream);
   if (rc == HS_OK)
     rc = launch_batch_expect(b->d_inst, b->ninst, b->max_n, b->d_partial, b->d_expect, b->stream);
   cudaMemcpyAsync(b->h_expect, b->d_expect, sizeof(double) * b->ninst, cudaMemcpyDeviceToHost,
@@ -411,10 +416,10 @@ int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* be
   // 1) one tile cap for every instance x CTAs per SM (up to the occupancy
   // limit) x tiles per work item
   double best = 1e300;
-  const int maxc = batch_max_ctas_per_sm();
+  const int maxc = 16;  // clamped to what fits an SM at launch
   int bc = b->tile_cap, bt = b->ctas_per_sm, bk = b->chunk;
   int bl = b->low_keep;
-  for (int cap : {9, 10, 11})
+  for (int cap : {9, 10, 11, 12})
     for (int low : {2, 3})
       for (int chunk : {4, 16}) {
         b->chunk = chunk;
@@ -443,7 +448,7 @@ int hs_batch_tune(hs_batch* b, int32_t* best_cap, int32_t* best_ctas, double* be
     if (n <= 9) continue;  // one pass whatever the cap
     const int keep = b->cap_of_n[n];
     int chosen = keep;
-    for (int cap : {9, 10, 11}) {
+    for (int cap : {9, 10, 11, 12}) {
       if (cap == (keep ? keep : bc)) continue;
       b->cap_of_n[n] = cap;
       if (build_plan(b) != HS_OK) continue;
@@ -476,9 +481,10 @@ int hs_batch_stats(hs_batch* b, int64_t* stats) {
   stats[1] = int64_t(b->ncounters);
   stats[2] = int64_t(b->pass_bytes);
   stats[3] = b->tile_cap;
-  stats[4] = std::min(b->ctas_per_sm, batch_max_ctas_per_sm());
+  stats[4] = std::min(b->ctas_per_sm, batch_max_ctas_per_sm(b->threads));
   stats[5] = b->chunk;
   stats[6] = b->low_keep;
+  stats[7] = b->threads;
   return HS_OK;
 }
 

@@ -182,9 +182,10 @@ int reduce_compare_count(const void* a, int adtype, const void* b, int bdtype, u
 constexpr int kBatchMaxQubits = 30;
 constexpr int kBatchMaxEdges = 64;
 constexpr int kBatchMaxRounds = 8;
-constexpr int kBatchMaxPasses = 4;   // passes per round (tile <= 11 bits, 8 new qubits each)
-constexpr int kBatchThreads = 128;   // 16 amplitudes per thread: tiles of up to 2^11
-constexpr int kBatchMaxTileBits = 11;
+constexpr int kBatchMaxPasses = 4;   // passes per round
+// 16 amplitudes per thread: CTAs of 128 threads take tiles of up to 2^11,
+// CTAs of 256 threads tiles of up to 2^12
+constexpr int kBatchMaxTileBits = 12;
 
 // one pass of a QAOA round over an instance: the tile bits, which of them get
 // the mixer RX, in register groups of 4 (tile-bit positions)
@@ -221,8 +222,8 @@ struct BatchItem {           // one (instance, step): its tiles in chunks, one w
 
 int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
                  int nitems_groups, uint64_t total_items, uint32_t* d_counters,
-                 unsigned long long* d_head, int* d_err, int grid, cudaStream_t s);
-int batch_max_ctas_per_sm();  // occupancy limit of the persistent kernel
+                 unsigned long long* d_head, int* d_err, int grid, int threads, cudaStream_t s);
+int batch_max_ctas_per_sm(int threads);  // occupancy limit of the persistent kernel
 int launch_batch_init(const BatchInstance* d_inst, int ninst, cudaStream_t s);
 int launch_batch_expect(const BatchInstance* d_inst, int ninst, int max_n, double* d_partial,
                         double* d_out, cudaStream_t s);

@@ -20,7 +20,7 @@
 namespace hisv {
 namespace {
 
-constexpr int kTileMax = 1 << kBatchMaxTileBits;
+// a CTA of NT threads holds tiles of up to 16 NT amplitudes (16 per thread)
 constexpr uint32_t kDepLimit = 1u << 24;  // polls (with ~0.1 us sleeps) before giving up
 
 __device__ __forceinline__ uint64_t bdep(uint64_t x, const Runs& r) {
@@ -43,12 +43,13 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+template <int NT>
 struct Shared {
-  alignas(16) uint8_t cut[kTileMax];
+  alignas(16) uint8_t cut[16 * NT];
   BatchPass pass;  // the item's pass, copied once per item
   float2 phase[kBatchMaxEdges + 1];
   uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
-  uint64_t gk[kTileMax / 2 / kBatchThreads];  // global offset of chunk k*threads
+  uint64_t gk[8];  // global offset of chunk k * NT
   int w[16];
   int c;
   int group;
@@ -57,7 +58,8 @@ struct Shared {
 };
 
 // w_q and C of the tile whose outer bits are gbase (warp 0 only)
-__device__ __forceinline__ void cross_weights(Shared& S, int nedges, int m, uint64_t gbase) {
+template <class Sh>
+__device__ __forceinline__ void cross_weights(Sh& S, int nedges, int m, uint64_t gbase) {
   const int lane = threadIdx.x & 31;
   if (lane < 16) S.w[lane] = 0;
   __syncwarp();
@@ -80,14 +82,17 @@ __device__ __forceinline__ void cross_weights(Shared& S, int nedges, int m, uint
   if (lane == 0) S.c = c;
 }
 
-__global__ void __launch_bounds__(kBatchThreads, 6)
+template <int NT>
+__global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
     k6_batch(const BatchInstance* __restrict__ insts, const BatchParams* __restrict__ pars,
              const BatchItem* __restrict__ groups, int ngroups, uint64_t total,
              uint32_t* __restrict__ counters, unsigned long long* __restrict__ head,
              int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kTileMax = 16 * NT;
+  constexpr int kBatchThreads = NT;
   float2* tiles = reinterpret_cast<float2*>(smem_raw);  // two buffers of kTileMax
-  Shared& S = *reinterpret_cast<Shared*>(smem_raw + 2 * kTileMax * sizeof(float2));
+  Shared<NT>& S = *reinterpret_cast<Shared<NT>*>(smem_raw + 2 * kTileMax * sizeof(float2));
   const int t = threadIdx.x;
   const uint32_t tiles_s = uint32_t(__cvta_generic_to_shared(tiles));
   for (;;) {
@@ -275,7 +280,10 @@ __global__ void __launch_bounds__(kBatchThreads, 6)
   }
 }
 
-constexpr size_t kBatchSmem = 2 * kTileMax * sizeof(float2) + sizeof(Shared);
+template <int NT>
+constexpr size_t batch_smem() {
+  return 2 * 16 * NT * sizeof(float2) + sizeof(Shared<NT>);
+}
 
 // |+>^n: every amplitude 2^(-n/2)
 __global__ void k6_init(const BatchInstance* __restrict__ insts) {
@@ -296,7 +304,7 @@ constexpr int kExpectBlocks = 256;
 
 __global__ void __launch_bounds__(256) k6_expect(const BatchInstance* __restrict__ insts,
                                                  double* __restrict__ partial) {
-  __shared__ Shared S;
+  __shared__ Shared<256> S;  // cut table for tiles of up to 2^12
   __shared__ double sh[8];
   const BatchInstance& I = insts[blockIdx.y];
   const int m = I.pass[0].m, nedges = I.nedges, t = threadIdx.x;
@@ -339,25 +347,39 @@ __global__ void k6_expect_finish(const double* __restrict__ partial, double* __r
 
 }  // namespace
 
-int batch_max_ctas_per_sm() {
+namespace {
+template <int NT>
+int max_ctas() {
   int n = 0;
-  if (cudaFuncSetAttribute(k6_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           int(kBatchSmem)) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k6_batch, kBatchThreads, kBatchSmem) !=
+  if (cudaFuncSetAttribute(k6_batch<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(batch_smem<NT>())) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k6_batch<NT>, NT, batch_smem<NT>()) !=
           cudaSuccess) {
     cudaGetLastError();
     return 1;
   }
   return n < 1 ? 1 : n;
 }
+}  // namespace
+
+int batch_max_ctas_per_sm(int threads) {
+  return threads == 256 ? max_ctas<256>() : max_ctas<128>();
+}
 
 int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
                  int ngroups, uint64_t total_items, uint32_t* d_counters,
-                 unsigned long long* d_head, int* d_err, int grid, cudaStream_t s) {
-  HS_CUDA(cudaFuncSetAttribute(k6_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(kBatchSmem)));
-  k6_batch<<<grid, kBatchThreads, kBatchSmem, s>>>(d_inst, d_par, d_items, ngroups, total_items,
-                                                   d_counters, d_head, d_err);
+                 unsigned long long* d_head, int* d_err, int grid, int threads, cudaStream_t s) {
+  if (threads == 256) {
+    HS_CUDA(cudaFuncSetAttribute(k6_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(batch_smem<256>())));
+    k6_batch<256><<<grid, 256, batch_smem<256>(), s>>>(d_inst, d_par, d_items, ngroups,
+                                                        total_items, d_counters, d_head, d_err);
+  } else {
+    HS_CUDA(cudaFuncSetAttribute(k6_batch<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(batch_smem<128>())));
+    k6_batch<128><<<grid, 128, batch_smem<128>(), s>>>(d_inst, d_par, d_items, ngroups,
+                                                        total_items, d_counters, d_head, d_err);
+  }
   HS_CUDA(cudaGetLastError());
   return HS_OK;
 }

@@ -289,8 +289,8 @@ int hs_batch_create_qaoa(int num_instances, const int32_t* num_qubits,
                          const double* gammas, const double* betas, hs_batch** out);
 /* New angles for the next run (the captured graph is reused). */
 int hs_batch_set_params(hs_batch* b, const double* gammas, const double* betas);
-/* Tile cap (6..11 qubits per pass) and persistent CTAs per SM (clamped to
- * what fits on an SM). */
+/* Tile cap (6..12 qubits per pass; a cap of 12 runs CTAs of 256 threads) and
+ * persistent CTAs per SM (clamped to what fits on an SM). */
 int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm);
 /* Tiles per work item (a dequeued chunk of one step of one instance). */
 int hs_batch_set_chunk(hs_batch* b, int tiles_per_item);
@@ -308,7 +308,7 @@ int hs_batch_tile_caps(hs_batch* b, int32_t* caps);
  * batch's stream, read-back of the results included (may be NULL). */
 int hs_batch_run(hs_batch* b, double* expect_out, double* ms);
 /* {work items, steps, bytes moved per run, tile cap, CTAs per SM, tiles per
- * item, lowest qubits kept in later passes' tiles} */
+ * item, lowest qubits kept in later passes' tiles, threads per CTA} */
 int hs_batch_stats(hs_batch* b, int64_t* stats);
 /* Complex64 amplitudes of one instance (qubit order) into host memory. */
 int hs_batch_state(hs_batch* b, int instance, void* host_out);

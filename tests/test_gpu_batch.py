@@ -50,7 +50,7 @@ def check_batch(batch, insts, states=True):
     return hc
 
 
-@pytest.mark.parametrize("cap", [9, 10, 11])
+@pytest.mark.parametrize("cap", [9, 10, 11, 12])
 def test_states_and_cost_vs_plain(cap):
     insts = make_instances([6, 7, 9, 12, 14, 16, 17, 21], 3, 500)
     b = abi.QaoaBatch([(n, e, g, bt) for n, e, g, bt, _ in insts], 3)
@@ -63,7 +63,8 @@ def test_states_and_cost_vs_plain(cap):
 def test_cta_schedules_agree(ctas):
     insts = make_instances([16, 18, 20, 22], 4, 900)
     b = abi.QaoaBatch([(n, e, g, bt) for n, e, g, bt, _ in insts], 4)
-    b.configure(11, 4)
+    b.configure(12, 4)
+    assert b.stats()["threads"] == 256
     base, _ = b.run()
     b.configure(10, ctas)
     b.set_chunk(3)
@@ -102,9 +103,9 @@ def test_tuner_and_mixed_sizes():
     insts = make_instances(ns, 4, 1234)
     b = abi.QaoaBatch([(n, e, g, bt) for n, e, g, bt, _ in insts], 4)
     cap, ctas, ms = b.tune()
-    assert cap in (9, 10, 11) and 1 <= ctas <= 16 and ms > 0
+    assert cap in (9, 10, 11, 12) and 1 <= ctas <= 16 and ms > 0
     caps = b.tile_caps()
-    assert set(caps.tolist()) <= {9, 10, 11}
+    assert set(caps.tolist()) <= {9, 10, 11, 12}
     st = b.stats()
     assert st["items"] > 0 and st["bytes_per_run"] > 0
     check_batch(b, insts, states=False)
