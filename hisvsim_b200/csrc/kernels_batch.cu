@@ -50,6 +50,7 @@ struct Shared {
   float2 phase[kBatchMaxEdges + 1];
   uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
   uint64_t gk[8];  // global offset of chunk k * NT
+  uint32_t gro[4];  // last group: global offset of each register bit
   int w[16];
   int c;
   int group;
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
     // thread bits of each register group: the tile bits not held in registers;
     // bswz is linear over GF(2), so a register element's slot is
     // bswz(thread part) ^ (XOR of bswz(register bit))
-    uint32_t sbase[3] = {0, 0, 0}, thr0 = 0;
+    uint32_t sbase[3] = {0, 0, 0}, thr0 = 0, thr_last = 0;
     for (int g = 0; g < ngr; ++g) {
       uint32_t rmask = 0, thr = 0;
       for (int j = 0; j < 4; ++j) rmask |= 1u << P.group_bits[g][j];
@@ -175,8 +176,14 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
         if (!((rmask >> b) & 1u)) thr |= uint32_t((t >> src++) & 1) << b;
       sbase[g] = bswz(thr);
       if (g == 0) thr0 = thr;
+      if (g == ngr - 1) thr_last = thr;
     }
-    __syncthreads();  // S.gk
+    // the last group writes its registers straight to global memory: the
+    // thread part's offset and each register bit's offset (disjoint bits add)
+    // (instances have at most 30 qubits, so offsets within a state fit 32 bits)
+    const uint32_t gl_base = uint32_t(bdep(thr_last, P.tile));
+    if (t < 4) S.gro[t] = uint32_t(bdep(1ull << P.group_bits[ngr - 1][t], P.tile));
+    __syncthreads();  // S.gk, S.gro
     // prologue: first tile into buffer 0
     {
       const uint64_t gb = bdep(t_begin, P.outer) + gt;
@@ -243,9 +250,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
             }
           }
           // mixer RX(2 beta) = [[c, -i s], [-i s, c]] on the group's target bits
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (!((P.group_rx[g] >> j) & 1)) continue;
+          auto rx_bit = [&](int j) {
 #pragma unroll
             for (int e0 = 0; e0 < 16; ++e0) {
               if ((e0 >> j) & 1) continue;
@@ -254,24 +259,48 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
               v[e0] = make_float2(rx.x * a.x + rx.y * b.y, rx.x * a.y - rx.y * b.x);
               v[e1] = make_float2(rx.y * a.y + rx.x * b.x, -rx.y * a.x + rx.x * b.y);
             }
+          };
+          const int gm = P.group_rx[g];
+          if (gm == 15) {  // the common case: all four register bits are targets
+            rx_bit(0);
+            rx_bit(1);
+            rx_bit(2);
+            rx_bit(3);
+          } else {
+            if (gm & 1) rx_bit(0);
+            if (gm & 2) rx_bit(1);
+            if (gm & 4) rx_bit(2);
+            if (gm & 8) rx_bit(3);
           }
+          if (g == ngr - 1) {
+            // last group: registers straight to global memory (the lanes run
+            // over the low, contiguous tile bits, so the stores coalesce)
+            float2* base = amp + gbase + gl_base;
+            uint32_t ro[4];
 #pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            uint32_t a = sbase[g];
+            for (int j = 0; j < 4; ++j) ro[j] = S.gro[j];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-              if ((e >> j) & 1) a ^= so[j];
-            tile[a] = v[e];
+            for (int e = 0; e < 16; ++e) {
+              uint32_t off = 0;
+#pragma unroll
+              for (int j = 0; j < 4; ++j)
+                if ((e >> j) & 1) off += ro[j];
+              base[off] = v[e];
+            }
+          } else {
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              uint32_t a = sbase[g];
+#pragma unroll
+              for (int j = 0; j < 4; ++j)
+                if ((e >> j) & 1) a ^= so[j];
+              tile[a] = v[e];
+            }
           }
         }
-        __syncthreads();
-      }
-      {
-        const uint64_t gb = gbase + gt;
-        for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads) {
-          const uint4 d = *reinterpret_cast<const uint4*>(&tile[bswz(2u * uint32_t(c))]);
-          *reinterpret_cast<uint4*>(amp + gb + S.gk[k]) = d;
-        }
+        // the next group reads what this one wrote; after the last group the
+        // next tile's first barrier protects the buffer
+        if (g < ngr - 1) __syncthreads();
       }
     }
     __threadfence();
