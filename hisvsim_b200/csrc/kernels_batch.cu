@@ -51,8 +51,8 @@ struct Shared {
   uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
   uint64_t gk[8];  // global offset of chunk k * NT
   uint32_t gro[4];  // last group: global offset of each register bit
-  int w[16];
-  int c;
+  int w[2][16];  // per tile buffer: warp 0 prepares the next tile's weights
+  int c[2];      // while the other warps may still read the current ones
   int group;
   int abort;
   unsigned long long item;
@@ -60,9 +60,10 @@ struct Shared {
 
 // w_q and C of the tile whose outer bits are gbase (warp 0 only)
 template <class Sh>
-__device__ __forceinline__ void cross_weights(Sh& S, int nedges, int m, uint64_t gbase) {
+__device__ __forceinline__ void cross_weights(Sh& S, int nedges, int m, uint64_t gbase, int buf) {
   const int lane = threadIdx.x & 31;
-  if (lane < 16) S.w[lane] = 0;
+  int* w = S.w[buf];
+  if (lane < 16) w[lane] = 0;
   __syncwarp();
   int c = 0;
   for (int e = lane; e < nedges; e += 32) {
@@ -73,14 +74,14 @@ __device__ __forceinline__ void cross_weights(Sh& S, int nedges, int m, uint64_t
       c += xa ^ xb;
     } else if (la && !lb) {
       c += xb;
-      atomicAdd(&S.w[a], xb ? -1 : 1);
+      atomicAdd(&w[a], xb ? -1 : 1);
     } else if (!la && lb) {
       c += xa;
-      atomicAdd(&S.w[b], xa ? -1 : 1);
+      atomicAdd(&w[b], xa ? -1 : 1);
     }
   }
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if (lane == 0) S.c = c;
+  if (lane == 0) S.c[buf] = c;
 }
 
 template <int NT>
@@ -195,19 +196,19 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
       const int buf = int(ti - t_begin) & 1;
       float2* tile = tiles + buf * kTileMax;
       const uint64_t gbase = bdep(ti, P.outer);
-      __syncthreads();  // the other buffer's previous tile is fully stored
+      cp_wait<0>();  // this tile's copies (the only ones in flight)
+      if (phase && t < 32) cross_weights(S, nedges, m, gbase, buf);
+      // one barrier per tile: every thread's copies and the weights are
+      // visible, and every thread is past the previous tile's last group,
+      // so the other buffer may be refilled
+      __syncthreads();
       if (ti + 1 < t_end) {
         const uint64_t nb = bdep(ti + 1, P.outer) + gt;
         const uint32_t ns = tiles_s + uint32_t((buf ^ 1) * kTileMax * 8);
         for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads)
           cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nb + S.gk[k]);
         cp_commit();
-        cp_wait<1>();
-      } else {
-        cp_wait<0>();
       }
-      if (phase && t < 32) cross_weights(S, nedges, m, gbase);
-      __syncthreads();
       for (int g = 0; g < ngr; ++g) {
         if (active) {
           uint32_t so[4];
@@ -224,14 +225,15 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
           }
           if (g == 0 && phase) {
             // cut = cut_low[i] + C + sum_q w_q i_q (tile bit q is qubit q)
-            int dthr = S.c;
+            const int* wt = S.w[buf];
+            int dthr = S.c[buf];
             for (int b = 0; b < m; ++b)
-              if ((thr0 >> b) & 1u) dthr += S.w[b];
+              if ((thr0 >> b) & 1u) dthr += wt[b];
             int wr[4];
             uint32_t rb[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-              wr[j] = S.w[P.group_bits[0][j]];
+              wr[j] = wt[P.group_bits[0][j]];
               rb[j] = 1u << P.group_bits[0][j];
             }
 #pragma unroll
@@ -346,13 +348,13 @@ __global__ void __launch_bounds__(256) k6_expect(const BatchInstance* __restrict
   double s = 0;
   for (uint64_t r = blockIdx.x; r < nranges; r += gridDim.x) {
     __syncthreads();
-    if (t < 32) cross_weights(S, nedges, m, r << m);
+    if (t < 32) cross_weights(S, nedges, m, r << m, 0);
     __syncthreads();
     const float2* a = I.amp + (r << m);
     for (int i = t; i < (1 << m); i += 256) {
-      int c = S.c + int(S.cut[i]);
+      int c = S.c[0] + int(S.cut[i]);
       for (int b = 0; b < m; ++b)
-        if ((i >> b) & 1) c += S.w[b];
+        if ((i >> b) & 1) c += S.w[0][b];
       const float2 v = a[i];
       s += (double(v.x) * v.x + double(v.y) * v.y) * double(c);
     }
