@@ -63,6 +63,7 @@ SIGNATURES = {
     "hs_part_run": [_vp, _vp, _i, _vp],
     "hs_parts_run": [_vp, _vp, _vp, _i, _vp],
     "hs_set_tile_qubits": [_i],
+    "hs_set_k1_reg_bits": [_i],
     "hs_plan_stats": [_i, _i, _vp, _i, _vp],
     "hs_fused_parts_run": [_vp, _vp, _vp, _i, _i, _vp],
     "hs_fused_compose": [_i, _vp, _vp, _i, _vp, _vp],
@@ -570,6 +571,14 @@ def fp64_peak_tflops() -> float:
 
 def set_tile_qubits(m: int) -> int:
     rc = lib().hs_set_tile_qubits(m)
+    if rc < 0:
+        check(rc)
+    return rc
+
+
+def set_k1_reg_bits(r: int) -> int:
+    """Amplitudes per thread (2^r, r = 3 or 4) of complex128 part passes."""
+    rc = lib().hs_set_k1_reg_bits(r)
     if rc < 0:
         check(rc)
     return rc

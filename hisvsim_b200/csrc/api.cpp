@@ -27,6 +27,8 @@ int set_error(int code, const char* fmt, ...) {
 static std::atomic<long long> g_gates{0}, g_passes{0}, g_param_bytes{0};
 static std::atomic<int> g_tile_hint{0};
 int current_tile_hint() { return g_tile_hint.load(); }
+static std::atomic<int> g_k1_rbits{3};
+int k1_reg_bits(int dtype) { return dtype == HS_DTYPE_C128 ? g_k1_rbits.load() : kRegBits; }
 
 // device-time accounting of K1/K2 launches: event pairs resolved when read
 static std::mutex g_ev_mu;
@@ -410,6 +412,11 @@ int hs_set_tile_qubits(int m) {
   if (m < 0 || m > kMaxTileBits) return set_error(HS_E_INVALID, "tile bits must be 0..%d",
                                                   kMaxTileBits);
   return g_tile_hint.exchange(m);
+}
+
+int hs_set_k1_reg_bits(int r) {
+  if (r != 3 && r != 4) return set_error(HS_E_INVALID, "K1 register bits must be 3 or 4");
+  return g_k1_rbits.exchange(r);
 }
 
 int hs_permute_bits(hs_state* st, const int32_t* pairs, int num_pairs, void* stream) {

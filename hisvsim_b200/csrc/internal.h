@@ -107,7 +107,7 @@ struct PartProgram {
   int32_t ngroups;
   int32_t nops;
   int32_t ncoef;
-  int32_t pad;
+  int32_t rbits;       // register bits of every group (amplitudes per thread = 2^rbits)
   uint64_t ntiles;     // 2^(n-m)
   Runs tile;           // tile index -> global index
   Runs outer;          // tile number -> global index
@@ -124,6 +124,10 @@ static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
               int tile_bits_hint, int dtype, std::vector<PartProgram>* programs);
 int current_tile_hint();  // hs_set_tile_qubits' value
+// register bits per thread of K1's complex128 programs (hs_set_k1_reg_bits:
+// 3 = 8 amplitudes (default), 4 = 16 amplitudes); complex64 programs always
+// use 4
+int k1_reg_bits(int dtype);
 // complex128 tiles stop at 2^11 so that three CTAs (two 32 KiB buffers each,
 // <= 168 registers per thread) share an SM; complex64 tiles go to 2^12
 inline int max_tile_bits(int dtype) { return dtype == HS_DTYPE_C64 ? 12 : 11; }

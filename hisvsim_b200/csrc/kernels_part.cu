@@ -356,22 +356,24 @@ __device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32
 }
 
 // complex64 tiles are at most 2^12 amplitudes: 2^(12-R) = 256 threads, one
-// CTA per SM bound; complex128 tiles at most 2^11: 128 threads, and the
-// register bound leaves room for three CTAs per SM (FP64-heavy passes need
-// the extra warps to hide latency)
-template <typename V>
+// CTA per SM bound; complex128 tiles at most 2^11: 128 threads of 16
+// amplitudes (R = 4) or 256 threads of 8 (R = 3), and the register bound
+// leaves room for three CTAs per SM (FP64-heavy passes need the extra warps
+// to hide latency; with two-qubit dense ops, R = 3 takes two CTAs of 256
+// threads so that the 4x4 bodies do not spill)
+template <typename V, int R, bool FULL>
 struct K1Threads {
   static constexpr int value = 256;
   static constexpr int min_blocks = 1;
 };
-template <>
-struct K1Threads<double2> {
-  static constexpr int value = 128;
-  static constexpr int min_blocks = 3;
+template <int R, bool FULL>
+struct K1Threads<double2, R, FULL> {
+  static constexpr int value = R == 3 ? 256 : 128;
+  static constexpr int min_blocks = (R == 3 && FULL) ? 2 : 3;
 };
 
 template <int R, bool FULL, typename V>
-__global__ void __launch_bounds__(K1Threads<V>::value, K1Threads<V>::min_blocks)
+__global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, FULL>::min_blocks)
     k1_part(V* __restrict__ sv, const __grid_constant__ PartProgram P) {
   using M = SmemMap<V>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -523,7 +525,7 @@ template <typename V>
 int launch_typed(V* a, const PartProgram& P, cudaStream_t s) {
   bool full = false;
   for (int i = 0; i < P.nops; ++i) full |= P.ops[i].kind == OP2_DENSE || P.ops[i].kind == OP2_SWAP;
-  const int R = P.m < kRegBits ? P.m : kRegBits;
+  const int R = P.rbits;
   if (full) {
     switch (R) {
       case 1: return launch_k1<1, true>(a, P, s);

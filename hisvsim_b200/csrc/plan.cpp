@@ -187,7 +187,11 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
   if (n < 1 || n > 63) return set_error(HS_E_INVALID, "bad qubit count %d", n);
   // two tile buffers must fit in shared memory: 2^12 complex128 / 2^13 complex64
   const int max_tile = std::min(n, max_tile_bits(dtype));
-  const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : max_tile);
+  // automatic size: the largest tile, except complex128 with 8 amplitudes per
+  // thread, whose 2^10 tiles (CTAs of 128 threads, six per SM) hide FP64
+  // latency better than 2^11 (measured)
+  const int auto_m = (dtype == HS_DTYPE_C128 && k1_reg_bits(dtype) == 3) ? 10 : max_tile;
+  const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : auto_m);
   // keep the lowest slots in the tile so that global accesses come in
   // contiguous runs of at least 64 bytes (complex64 tiles also need slot 0 for
   // their 16-byte chunks)
@@ -235,7 +239,7 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
     for (int s = 0; s < n && int(tile.size()) < m; ++s)
       if (std::find(tile.begin(), tile.end(), s) == tile.end()) tile.push_back(s);
     std::sort(tile.begin(), tile.end());
-    const int R = std::min(kRegBits, m);
+    const int R = std::min(k1_reg_bits(dtype), m);
     std::vector<int> tbit_of_slot(n, -1);
     for (int i = 0; i < m; ++i) tbit_of_slot[tile[i]] = i;
     PartProgram* P = nullptr;
@@ -246,6 +250,7 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       P->n = n;
       P->m = m;
       P->ntiles = 1ull << (n - m);
+      P->rbits = R;
       build_runs(tile, &P->tile);
       for (int b = 0; b < m; ++b) P->tile_slot[b] = uint8_t(tile[b]);
       std::vector<int> outer;

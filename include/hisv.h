@@ -180,6 +180,11 @@ int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates
 
 /* Tile-size override for K1 (0 = automatic).  Returns the previous value. */
 int hs_set_tile_qubits(int m);
+/* Amplitudes per thread of K1's complex128 passes: 2^r with r = 3 (default;
+ * automatic tiles of 2^10 in CTAs of 128 threads, six per SM) or 4 (tiles of
+ * 2^11 in CTAs of 128 threads, three per SM).  Complex64 passes always hold
+ * 16.  Returns the previous value. */
+int hs_set_k1_reg_bits(int r);
 
 /* ---- precision form (complex64 state, fused unitaries on the tensor cores) --
  * No counterpart in the reference: each part (<= 6 qubits) becomes one 64x64

@@ -68,6 +68,30 @@ def test_tile_sizes(port, m):
         abi.set_tile_qubits(prev)
 
 
+@pytest.mark.parametrize("r,m", [(3, 3), (3, 5), (3, 9), (3, 11), (4, 4), (4, 9), (4, 11)])
+def test_amplitudes_per_thread(port, r, m):
+    """complex128 passes with 8 (r = 3, the default) or 16 (r = 4) amplitudes
+    per thread give the oracle's result, with and without two-qubit dense ops."""
+    n = 14
+    gates = all_gates(n, 140, 31 + m)
+    want = port.run(n, to_records(gates))
+    prev_m = abi.set_tile_qubits(m)
+    prev_r = abi.set_k1_reg_bits(r)
+    try:
+        st = abi.State(n)
+        st.run_part(gates)
+        assert np.abs(st.amplitudes() - want).max() <= TOL
+        u3 = circuits.random_u3_cz(n, 6, 5)
+        parts = partition.partition_dfs(u3, 9)
+        rec, offs = part_offsets(partition.parts_to_gates(u3, parts))
+        st.set_basis(0)
+        st.run_parts(rec, offs)
+        assert np.abs(st.amplitudes() - port.run(n, to_records(u3))).max() <= TOL
+    finally:
+        abi.set_tile_qubits(prev_m)
+        abi.set_k1_reg_bits(prev_r)
+
+
 def test_config0_20q_against_reference(ref):
     """20 qubits, 20 random layers, acyclic parts of <= 10 qubits."""
     gates = circuits.random_layered(20, 20, 0)
