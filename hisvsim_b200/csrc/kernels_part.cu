@@ -387,8 +387,18 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   // of k*nthr are disjoint, so deposit(c << SH) = deposit(t << SH) + deposit(k*nthr << SH).
   const int nchunk = (1 << P.m) >> M::SH;
   const int per_thr = nchunk / int(nthr);
+  // the last group writes its registers straight to global memory: the global
+  // offset of each of its register bits and of each thread's thread part
+  // (after the chunk table; kept in shared memory to spare registers)
+  uint64_t* s_glreg = s_gchunk + per_thr;
+  uint64_t* s_glthr = s_glreg + R;
+  const GroupDesc& GL = P.groups[P.ngroups - 1];
   for (int k = t; k < per_thr; k += nthr)
     s_gchunk[k] = deposit(uint64_t(k) * nthr << M::SH, P.tile);
+  for (int j = int(t); j < R; j += int(nthr)) s_glreg[j] = deposit(1ull << GL.reg_tbit[j], P.tile);
+  // (the last group's lanes run over the lowest tile bits, so the direct
+  // stores coalesce)
+  s_glthr[t] = deposit(deposit(t, GL.thr), P.tile);
   __syncthreads();
   const uint64_t gt = deposit(uint64_t(t) << M::SH, P.tile);
   const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(buf[0]));
@@ -398,19 +408,24 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   if (tile < P.ntiles)
     issue_tile_load<R, V>(sv, sb0, deposit(tile, P.outer), s_gchunk, gt, per_thr);
   cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
   V v[E], w[E];
   for (int it = 0; tile < P.ntiles; ++it, tile += gridDim.x) {
+    // this tile has landed and every thread is past the previous one (the
+    // barrier that ends the previous tile's last group), so the previous
+    // tile's buffer may take the next tile
     const uint64_t next = tile + gridDim.x;
-    if (next < P.ntiles)
+    if (next < P.ntiles) {
       issue_tile_load<R, V>(sv, (it & 1) ? sb0 : sb1, deposit(next, P.outer), s_gchunk, gt,
                             per_thr);
-    cp_async_commit();
-    cp_async_wait<1>();  // this tile's copies (all but the newest group) have landed
-    __syncthreads();
+      cp_async_commit();
+    }
     unsigned char* A = buf[it & 1];
     const uint64_t gbase = deposit(tile, P.outer);
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
+      const bool last = g == P.ngroups - 1;
       const uint32_t thr = uint32_t(deposit(t, G.thr));
       // per register bit: the offset change of setting that bit (swizzled slot
       // part and in-slot part occupy disjoint bits, so they combine by XOR and
@@ -427,6 +442,30 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
         a[0] = sthr;
 #pragma unroll
         for (int e = 1; e < E; ++e) a[e] = a[e & (e - 1)] ^ dx[lowest_bit(e)];
+      };
+      // the group's result: to shared memory for the next group, or (last
+      // group) straight to global memory, each element's offset a sum of
+      // disjoint bit parts
+      auto finish = [&](const V (&x)[E]) {
+        if (last) {
+          // elements in Gray-code order: each address is the previous one
+          // plus or minus one register bit's offset (one live pointer)
+          V* p = sv + gbase + s_glthr[t];
+#pragma unroll
+          for (int i = 0; i < E; ++i) {
+            const int e = i ^ (i >> 1);
+            if (i > 0) {
+              const int j = lowest_bit(i);
+              if ((e >> j) & 1) p += s_glreg[j]; else p -= s_glreg[j];
+            }
+            __stcs(p, x[e]);
+          }
+        } else {
+          uint32_t a[E];
+          offsets(a);
+#pragma unroll
+          for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + a[e]) = x[e];
+        }
       };
       {
         uint32_t a[E];
@@ -449,12 +488,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
         op_inplace<R, FULL>(v, op, P.coef + op.coef, thr, gbase, dfr);
       }
       apply_deferred<R>(v, dfr);
-      {
-        uint32_t a[E];
-        offsets(a);
-#pragma unroll
-        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + a[e]) = v[e];
-      }
+      finish(v);
       goto group_done;
     in_w:
       while (o < o_end) {
@@ -466,22 +500,14 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
         op_inplace<R, FULL>(w, op, P.coef + op.coef, thr, gbase, dfr);
       }
       apply_deferred<R>(w, dfr);
-      {
-        uint32_t a[E];
-        offsets(a);
-#pragma unroll
-        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(A + a[e]) = w[e];
-      }
+      finish(w);
     group_done:
-      __syncthreads();  // the group's writes precede the next group's reads
+      // the group's writes precede the next group's reads; after the last
+      // group the next tile's copies (the only ones in flight) must have
+      // landed and every thread must be done with this tile's buffer
+      if (last) cp_async_wait<0>();
+      __syncthreads();
     }
-    // write the tile back: chunk c = t + k*nthr, coalesced 16-byte stores
-    for (int k = 0; k < per_thr; ++k) {
-      const uint32_t c = t + uint32_t(k) * nthr;
-      const uint4 d = *reinterpret_cast<const uint4*>(A + (swz(c) << 4));
-      __stcs(reinterpret_cast<uint4*>(sv + gbase + gt + s_gchunk[k]), d);
-    }
-    __syncthreads();  // buffer A is free for the prefetch issued next iteration
   }
   cp_async_wait<0>();
 }
@@ -507,7 +533,7 @@ int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
   if (g_num_sms == 0) HS_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
   const int threads = 1 << (P.m - R);
   const int per_thr = ((1 << P.m) * int(sizeof(V)) / 16) / threads;
-  const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(uint64_t) * per_thr;
+  const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(uint64_t) * (per_thr + R + threads);
   if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K1 tile of 2^%d needs %zu B", P.m, smem);
   int per_sm = 0;
   HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, V>, threads, smem));
