@@ -433,9 +433,12 @@ def main():
         fpasses = cf["passes"] / args.steps
         fbytes = 2.0 * (1 << n) * 8
         k4_ms = cf["apply_us"] / 1e3 / max(1, cf["passes"])
-        shape = abi.set_fused_shape(1, 13)
+        shape = abi.set_fused_shape(1, 12)
         abi.set_fused_shape(shape // 100, shape % 100)
-        kname = "k4_direct" if shape // 100 == 1 else "k4_fused"
+        variant = abi.set_k4_variant(2)
+        abi.set_k4_variant(variant)
+        kname = ({0: "k4_direct", 1: "k4_ws", 2: "k4_bulk"}[variant] if shape // 100 == 1
+                 else "k4_fused")
         # tensor work: three BF16 products of a 128 x 128 real GEMM per amplitude column
         tflops = 3 * 8.0 * 64 * (1 << n) * fpasses / t_f / 1e12
         fused = {"circuit_s": t_f, "parts": len(fparts), "passes_per_step": fpasses,

@@ -116,7 +116,7 @@ void runs_of(const std::vector<int>& dst, Runs* r) {
 // passes for the fused unitaries: consecutive parts whose slots (plus the two
 // lowest slots) fit a tile of 2^12 amplitudes, at most kFusedMaxOps per pass
 // pass shape: unitaries per state pass and tile bits (hs_set_fused_shape)
-std::atomic<int> g_fused_ops{1}, g_fused_bits{13};
+std::atomic<int> g_fused_ops{1}, g_fused_bits{12};
 
 int plan_fused(int n, const std::vector<int>& q2s, const std::vector<PartLocal>& parts,
                int precision, std::vector<FusedPass>* out) {
@@ -250,7 +250,7 @@ int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int pre
 }
 
 int hs_set_k4_variant(int variant) {
-  if (variant < 0 || variant > 1) return set_error(HS_E_INVALID, "K4 variant 0 or 1");
+  if (variant < 0 || variant > 2) return set_error(HS_E_INVALID, "K4 variant 0, 1 or 2");
   return set_k4_variant(variant);
 }
 

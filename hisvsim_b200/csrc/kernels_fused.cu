@@ -11,6 +11,7 @@
 // Ah*Bh + Ah*Bl + Al*Bh (the Al*Bl term, ~2^-16 relative, is dropped).
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include "internal.h"
@@ -708,9 +709,293 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4DirectCols);
 }
 
+// ---- K4, one unitary per pass, bulk-loaded ----------------------------------------
+// The warp-specialised pipeline with a fourth role: a loader warp brings
+// whole tiles into shared memory with bulk copies (cp.async.bulk, completing
+// on an mbarrier with a byte count), so the HBM reads in flight are not
+// bounded by the producers' registers or per-thread load slots.  A raw
+// complex64 tile and its BF16 hi / lo B operand have the same size, so each
+// of the four buffers holds tile i first raw, then as B:
+//   warp 17     loader: for tile i, once the MMAs of tile i-4 have read
+//               buffer i%4 (bfree), arm rfull(i%4) with the tile's byte count
+//               and copy the tile's contiguous runs (the lowest run of tile
+//               bits, slots 0..L0-1) in tile-index order;
+//   warps 0-7   producers: wait rfull(i%4), read their raw amplitudes into
+//               registers, meet at a named barrier (every raw read precedes
+//               every B write), write the BF16 hi / lo rows, arrive on
+//               bfull(i%4);
+//   warp 16     MMA issue (commits to mdone(i%2) and bfree(i%4));
+//   warps 8-15  epilogue: TMEM -> registers -> a per-warp shared-memory
+//               transpose -> 16-byte stores, each lane writing two amplitudes
+//               that are adjacent in memory, the lanes of a store covering
+//               contiguous runs.
+// Three tiles are in flight while one is converted.  Tiles up to 2^12
+// amplitudes.
+constexpr int kBulkThreads = 576;  // 8 producer, 8 epilogue, 1 MMA, 1 loader warps
+constexpr int kBulkItems = 4;      // B items per producer thread (N * 16 / 256, N <= 64)
+constexpr int kBulkBuffers = 4;
+constexpr int kBulkMaxChunkBits = 9;  // bulk copies of at most 2^9 amplitudes (4 KiB)
+constexpr int kBulkStageFloats = 512;  // per epilogue warp: 16 p x 16 columns x (re, im)
+
+__global__ void __launch_bounds__(kBulkThreads, 1)
+    k4_bulk(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
+            const uint8_t* __restrict__ a_all, int* __restrict__ err, int chunk_bits) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m = P.m, T = 1 << m;
+  const int N = 1 << (m - kFusedBits);
+  const int lgN = m - kFusedBits;
+  const uint32_t bk = uint32_t(N) * 16u;
+  const uint32_t bbytes = uint32_t(N) * 256u;
+  const int nchunks = T >> chunk_bits;
+  const uint32_t chunk_bytes = 8u << chunk_bits;
+  uint8_t* sA = sm;
+  uint8_t* sB = sA + kFusedABytes;  // [kBulkBuffers][T * 8 bytes]: raw tile, then hi | lo
+  uint64_t* gp = reinterpret_cast<uint64_t*>(sB + kBulkBuffers * size_t(T) * 8);
+  uint64_t* gn = gp + 64;
+  uint64_t* gc = gn + N;                                     // global offset of chunk c
+  uint32_t* tq = reinterpret_cast<uint32_t*>(gc + nchunks);  // tile index of part index p
+  uint32_t* tn = tq + 64;                                    // tile index of column n
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tn + N);
+  uint64_t* rfull = bars;                  // [kBulkBuffers]
+  uint64_t* bfull = rfull + kBulkBuffers;  // [kBulkBuffers]
+  uint64_t* bfree = bfull + kBulkBuffers;  // [kBulkBuffers]
+  uint64_t* mdone = bfree + kBulkBuffers;  // [2]
+  uint64_t* tfree = mdone + 2;             // [2]
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tfree + 2);
+  uint32_t* tmem_base = reinterpret_cast<uint32_t*>(tfree + 3);
+  float* stage = reinterpret_cast<float*>(tfree + 4);  // [8 warps][kBulkStageFloats]
+
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a_all + size_t(P.part[0]) * kFusedABytes);
+    uint4* dst = reinterpret_cast<uint4*>(sA);
+    for (int i = t; i < kFusedABytes / 16; i += kBulkThreads) dst[i] = src[i];
+  }
+  uint32_t pmask = 0;
+  for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[0][b];
+  for (int p = t; p < 64; p += kBulkThreads) {
+    uint32_t x = 0;
+    for (int b = 0; b < kFusedBits; ++b) x |= uint32_t((p >> b) & 1) << P.pbits[0][b];
+    tq[p] = x;
+    gp[p] = dep(x, P.tile);
+  }
+  for (int nn = t; nn < N; nn += kBulkThreads) {
+    uint32_t x = 0;
+    int bit = 0;
+    for (int b = 0; b < m; ++b)
+      if (!((pmask >> b) & 1)) x |= uint32_t((nn >> bit++) & 1) << b;
+    tn[nn] = x;
+    gn[nn] = dep(x, P.tile);
+  }
+  for (int c = t; c < nchunks; c += kBulkThreads) gc[c] = dep(uint64_t(c) << chunk_bits, P.tile);
+  if (t == 0) {
+    for (int b = 0; b < kBulkBuffers; ++b) {
+      tc::mbar_init(&rfull[b], 1);
+      tc::mbar_init(&bfull[b], kWsProducers);
+      tc::mbar_init(&bfree[b], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&mdone[b], 1);
+      tc::mbar_init(&tfree[b], kWsProducers);  // the epilogue has as many threads
+    }
+    *abort_flag = 0;
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_base, 2 * kK4DirectCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_base;
+  const uint64_t cnt =
+      blockIdx.x < P.ntiles ? (P.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto tile_of = [&](uint64_t i) { return blockIdx.x + i * gridDim.x; };
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicExch(err, 1);
+  };
+
+  if (warp == 17) {
+    // ---- loader
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i % kBulkBuffers);
+      if (i >= kBulkBuffers &&
+          !tc::mbar_wait(&bfree[b], uint32_t(i / kBulkBuffers - 1) & 1u, kWaitLimit)) {
+        fail();
+        break;
+      }
+      if (lane == 0) tc::mbar_arrive_expect_tx(&rfull[b], uint32_t(T) * 8u);
+      __syncwarp();
+      const float2* base = sv + dep(tile_of(i), P.outer);
+      const uint32_t dst = tc::smem_u32(sB + size_t(b) * T * 8);
+      for (int c = lane; c < nchunks; c += 32)
+        tc::bulk_load(dst + uint32_t(c) * chunk_bytes, base + gc[c], chunk_bytes, &rfull[b]);
+      issued = i + 1;
+    }
+    // no copy may still be landing when the CTA leaves: wait for the last
+    // tile of each buffer (its phase is that buffer's latest)
+    for (uint64_t j = issued > kBulkBuffers ? issued - kBulkBuffers : 0; j < issued; ++j)
+      tc::mbar_wait(&rfull[j % kBulkBuffers], uint32_t(j / kBulkBuffers) & 1u, kWaitLimit);
+  } else if (warp < 8) {
+    // ---- producers: item k is amplitudes p = 4kb..4kb+3 of column nn
+    const int nitems = (N * 16) / kWsProducers;  // 1..4
+    uint32_t roff[kBulkItems][4];  // byte offsets in the raw tile
+    uint32_t boff[kBulkItems];     // byte offset of the item's B row
+#pragma unroll
+    for (int k = 0; k < kBulkItems; ++k) {
+      const int item = (t + k * kWsProducers) & ((N * 16) - 1);
+      const int kb = item >> lgN, nn = item & (N - 1);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) roff[k][q] = (tq[4 * kb + q] | tn[nn]) * 8u;
+      boff[k] = tc::kmajor_off(uint32_t(nn), uint32_t(kb * 8), bk);
+    }
+    for (uint64_t i = 0; i < cnt; ++i) {
+      const int b = int(i % kBulkBuffers);
+      const bool ok =
+          !*abort_flag && tc::mbar_wait(&rfull[b], uint32_t(i / kBulkBuffers) & 1u, kWaitLimit);
+      if (!ok) fail();
+      uint8_t* buf = sB + size_t(b) * T * 8;
+      float2 x[kBulkItems][4];
+#pragma unroll
+      for (int k = 0; k < kBulkItems; ++k) {
+        if (k >= nitems) break;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[k][q] = *reinterpret_cast<const float2*>(buf + roff[k][q]);
+      }
+      // every raw read precedes every B write; the producers leave together
+      // (a vote at the same named barrier) when any of them saw a timeout or
+      // the abort word
+      uint32_t stop;
+      asm volatile(
+          "{\n .reg .pred p, q;\n setp.eq.u32 p, %1, 0;\n"
+          " bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+          : "=r"(stop)
+          : "r"(uint32_t(ok)), "n"(kWsProducers)
+          : "memory");
+      if (stop) break;
+      uint8_t* bl = buf + bbytes;
+#pragma unroll
+      for (int k = 0; k < kBulkItems; ++k) {
+        if (k >= nitems) break;
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x[k][q].x, x[k][q].y);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(x[k][q].x - hf.x, x[k][q].y - hf.y);
+          hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+          lw[q] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+        *reinterpret_cast<uint4*>(buf + boff[k]) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(bl + boff[k]) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+      }
+      tc::fence_proxy_async_smem();  // the B writes become visible to the tensor cores
+      mbar_arrive(&bfull[b]);
+    }
+  } else if (warp < 16) {
+    // ---- epilogue: TMEM accumulator -> shared-memory transpose -> HBM.
+    // Thread (quad, lane) holds real-form row r = 32 quad + lane, i.e. the
+    // re (lane even) or im part of part index p = 16 quad + lane / 2.  Per
+    // chunk of 16 columns the warp writes its 16 p x 16 columns x (re, im)
+    // to its staging block (column pairs XOR-swizzled by p, so the writes
+    // spread over the banks and a column pair stays one 16-byte slot), then
+    // stores two memory-adjacent amplitudes per lane: (p; c, c+1) when
+    // column bit 0 is slot 0, else (p, p+1; c) (part bit 0 is slot 0).
+    const int quad = warp & 3, half = (warp - 8) >> 2;
+    const int comp = lane & 1, pl = lane >> 1;
+    const bool pairs = (gn[1] == 1);
+    const int per = N / 2 < 16 ? 16 : N / 2;
+    const int c_begin = half * per;
+    const int c_end = c_begin + per < N ? c_begin + per : N;
+    float* stg = stage + (warp - 8) * kBulkStageFloats;
+    auto sidx = [](int p, int c) { return p * 32 + ((c ^ ((p & 7) << 1)) << 1); };
+    const uint64_t* gpq = gp + quad * 16;
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i & 1);
+      if (!tc::mbar_wait(&mdone[b], uint32_t(i >> 1) & 1u, kWaitLimit)) {
+        fail();
+        break;
+      }
+      tc::tc_fence_after();
+      float2* tb = sv + dep(tile_of(i), P.outer);
+      for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
+        float d[16];
+        tc::tmem_ld16(tmem + uint32_t(b) * kK4DirectCols + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
+        __syncwarp();  // the previous chunk's staging reads are done
+#pragma unroll
+        for (int c = 0; c < 16; ++c) stg[sidx(pl, c) + comp] = d[c];
+        __syncwarp();
+        if (pairs) {
+#pragma unroll
+          for (int s4 = 0; s4 < 4; ++s4) {
+            const int p = (lane >> 3) + 4 * s4, c = 2 * (lane & 7);
+            const float4 v = *reinterpret_cast<const float4*>(stg + sidx(p, c));
+            __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]), v);
+          }
+        } else {
+#pragma unroll
+          for (int s4 = 0; s4 < 4; ++s4) {
+            const int p = 2 * ((lane >> 4) + 2 * s4), c = lane & 15;
+            const float2 lo = *reinterpret_cast<const float2*>(stg + sidx(p, c));
+            const float2 hi = *reinterpret_cast<const float2*>(stg + sidx(p + 1, c));
+            __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]),
+                   make_float4(lo.x, lo.y, hi.x, hi.y));
+          }
+        }
+      }
+      tc::tc_fence_before();
+      mbar_arrive(&tfree[b]);
+    }
+  } else if (warp == 16 && lane == 0) {
+    // ---- MMA issue
+    const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
+    const int nprod = P.precision == 1 ? 1 : 3;
+    const uint32_t a0 = tc::smem_u32(sA);
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i & 1);
+      const int bb = int(i % kBulkBuffers);
+      if (!tc::mbar_wait(&bfull[bb], uint32_t(i / kBulkBuffers) & 1u, kWaitLimit) ||
+          (i >= 2 && !tc::mbar_wait(&tfree[b], uint32_t((i - 2) >> 1) & 1u, kWaitLimit))) {
+        fail();
+        break;
+      }
+      tc::tc_fence_after();
+      const uint32_t bhs = tc::smem_u32(sB + size_t(bb) * T * 8), bls = bhs + bbytes;
+      const uint32_t d = tmem + uint32_t(b) * kK4DirectCols;
+      uint32_t acc = 0;
+      for (int prod = 0; prod < nprod; ++prod) {
+        const uint32_t abase = a0 + (prod == 2 ? uint32_t(kFusedABytes / 2) : 0u);
+        const uint32_t bbase = prod == 1 ? bls : bhs;
+        for (int s = 0; s < 8; ++s) {
+          const uint64_t ad = tc::smem_desc(abase + uint32_t(s) * 2u * 2048u, 2048u, 128u);
+          const uint64_t bd = tc::smem_desc(bbase + uint32_t(s) * 2u * bk, bk, 128u);
+          tc::mma_bf16(d, ad, bd, idesc, acc);
+          acc = 1;
+        }
+      }
+      tc::mma_commit(&mdone[b]);
+      tc::mma_commit(&bfree[bb]);  // buffer bb may take tile i+4
+      issued = i + 1;
+    }
+    // the last committed MMAs complete before TMEM is released
+    if (issued > 0) {
+      const uint64_t j = issued - 1;
+      tc::mbar_wait(&mdone[j & 1], uint32_t(j >> 1) & 1u, kWaitLimit);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4DirectCols);
+}
+
 }  // namespace
 
-std::atomic<int> g_k4_variant{1};  // one unitary per pass: 0 direct, 1 warp-specialised
+// one unitary per pass: 0 direct, 1 warp-specialised, 2 bulk-loaded (default)
+std::atomic<int> g_k4_variant{2};
 
 int set_k4_variant(int v) { return g_k4_variant.exchange(v); }
 
@@ -743,7 +1028,37 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     attr = true;
   }
   const int T = 1 << P.m, N = T >> kFusedBits;
-  if (P.nops == 1 && g_k4_variant.load() == 1) {
+  const int variant = g_k4_variant.load();
+  // the bulk form copies the lowest run of tile bits (slot 0 upward) and
+  // stores two memory-adjacent amplitudes per lane: slot 0 must be tile bit
+  // 0 and, when it belongs to the part, its local bit 0
+  bool bulk = P.nops == 1 && variant == 2 && P.m <= 12 && P.tile.n > 0 && P.tile.src[0] == 0 &&
+              P.tile.dst[0] == 0 && P.tile.len[0] >= 2;
+  for (int j = 1; j < kFusedBits; ++j) bulk = bulk && P.pbits[0][j] != 0;
+  if (bulk) {
+    // A, four raw / B buffers, offset tables, sixteen mbarriers, the abort
+    // word, the TMEM address and the epilogue's staging blocks
+    static bool battr = false;
+    if (!battr) {
+      HS_CUDA(cudaFuncSetAttribute(k4_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+      battr = true;
+    }
+    const int chunk_bits = std::min<int>(P.tile.len[0], kBulkMaxChunkBits);
+    const int nchunks = T >> chunk_bits;
+    const size_t bsmem = size_t(kFusedABytes) + size_t(T) * 8 * kBulkBuffers + 64 * 8 +
+                         size_t(N) * 8 + size_t(nchunks) * 8 + 64 * 4 + size_t(N) * 4 +
+                         20 * 8 + 8 * kBulkStageFloats * 4;
+    if (bsmem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 bulk pass needs %zu B", bsmem);
+    int bsms = 148, bdev = 0;
+    HS_CUDA(cudaGetDevice(&bdev));
+    HS_CUDA(cudaDeviceGetAttribute(&bsms, cudaDevAttrMultiProcessorCount, bdev));
+    const int bgrid = int(P.ntiles < uint64_t(bsms) ? P.ntiles : uint64_t(bsms));
+    k4_bulk<<<bgrid, kBulkThreads, bsmem, s>>>(static_cast<float2*>(amp), P,
+                                               static_cast<const uint8_t*>(d_a), d_err, chunk_bits);
+    HS_CUDA(cudaGetLastError());
+    return HS_OK;
+  }
+  if (P.nops == 1 && variant >= 1) {
     // warp-specialised form: A, two B buffers, offset tables, six mbarriers
     static bool wattr = false;
     if (!wattr) {

@@ -125,14 +125,28 @@ def test_fused_pass_shapes(port, shape):
     assert np.abs(got - want).max() <= 1e-5
 
 
-def test_fused_apply_given_unitary():
+@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("qubits", [[11, 0, 5, 3, 9, 7], [0, 11, 5, 3, 9, 7], [12, 2, 5, 3, 9, 7],
+                                    [1, 2, 3, 4, 5, 6]])
+def test_fused_apply_given_unitary(variant, qubits):
     """hs_fused_apply with a random 64x64 unitary on scattered qubits, against
-    numpy on the complex128 amplitudes."""
-    n = 12
+    numpy on the complex128 amplitudes: slot 0 as a later local bit (the
+    bulk-loaded kernel hands such passes to the warp-specialised one), as
+    local bit 0, outside the unitary, and a unitary on slots 1-6."""
+    n = 13
     rng = np.random.default_rng(4)
     z = rng.normal(size=(64, 64)) + 1j * rng.normal(size=(64, 64))
     u, _ = np.linalg.qr(z)
-    qubits = [11, 0, 5, 3, 9, 7]
+    prev = abi.set_k4_variant(variant)
+    shape = abi.set_fused_shape(1, 12)  # the bulk-loaded kernel takes tiles up to 2^12
+    try:
+        _apply_and_check(n, u, qubits)
+    finally:
+        abi.set_k4_variant(prev)
+        abi.set_fused_shape(shape // 100, shape % 100)
+
+
+def _apply_and_check(n, u, qubits):
     st = abi.State(n, abi.C64)
     gates = circuits.random_u3_cz(n, 3, 8)
     for g in gates:
@@ -150,21 +164,24 @@ def test_fused_apply_given_unitary():
     assert np.abs(got - want).max() <= 1e-5
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant,bits", [(0, 13), (1, 13), (1, 12), (2, 10), (2, 11), (2, 12)])
 @pytest.mark.parametrize("n", [10, 13, 17])
-def test_k4_variants(port, variant, n):
-    """Both one-unitary-per-pass kernels (direct, warp-specialised) agree with
-    the oracle, including states with fewer tiles than SMs."""
+def test_k4_variants(port, variant, bits, n):
+    """The one-unitary-per-pass kernels (direct, warp-specialised,
+    bulk-loaded) agree with the oracle, including states with fewer tiles
+    than SMs."""
     gates = circuits.random_u3_cz(n, 6, 23)
     parts = partition.partition_dfs(gates, 6)
     rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
     want = port.run(n, to_records(gates))
     prev = abi.set_k4_variant(variant)
+    shape = abi.set_fused_shape(1, bits)
     try:
         st = abi.State(n, abi.C64)
         st.run_fused(rec, offs, 0)
         got = st.amplitudes().astype(complex)
     finally:
         abi.set_k4_variant(prev)
+        abi.set_fused_shape(shape // 100, shape % 100)
     assert 1 - fid(want, got) <= 1e-8
     assert np.abs(got - want).max() <= 1e-5
