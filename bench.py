@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--cpu-layers", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--tile-qubits", type=int, default=11, help="K1 tile bits (0 = automatic)")
+    ap.add_argument("--tile-qubits", type=int, default=0, help="K1 tile bits (0 = automatic)")
     ap.add_argument("--no-fused", action="store_true", help="skip the precision form")
     ap.add_argument("--fused-shape", default="",
                     help="unitaries per pass and tile bits of the precision form, e.g. 2,12")
@@ -587,7 +587,8 @@ def main():
                                    f"(U3 all qubits + CZ random matching), plain complex128",
                        "gates": len(gates), "parts": len(parts),
                        "part_qubits": args.part_qubits, "partitioner": args.partitioner,
-                       "tile_qubits": args.tile_qubits,
+                       "tile_qubits": args.tile_qubits or "automatic (2^10 tiles, 8 amplitudes "
+                                                          "per thread for complex128)",
                        "passes_per_step": passes, "state_bytes": (1 << n) * 16,
                        "l2": "state >> L2 (126 MB), no flush", "parallelism": f"replicas{world}"},
             "circuit_s": t_step, "hbm_GBps": passes * bytes_per_pass / t_step / 1e9,
