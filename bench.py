@@ -433,7 +433,7 @@ def main():
         fpasses = cf["passes"] / args.steps
         fbytes = 2.0 * (1 << n) * 8
         k4_ms = cf["apply_us"] / 1e3 / max(1, cf["passes"])
-        shape = abi.set_fused_shape(1, 12)
+        shape = abi.set_fused_shape(1, 13)
         abi.set_fused_shape(shape // 100, shape % 100)
         variant = abi.set_k4_variant(2)
         abi.set_k4_variant(variant)

@@ -116,7 +116,7 @@ void runs_of(const std::vector<int>& dst, Runs* r) {
 // passes for the fused unitaries: consecutive parts whose slots (plus the two
 // lowest slots) fit a tile of 2^12 amplitudes, at most kFusedMaxOps per pass
 // pass shape: unitaries per state pass and tile bits (hs_set_fused_shape)
-std::atomic<int> g_fused_ops{1}, g_fused_bits{12};
+std::atomic<int> g_fused_ops{1}, g_fused_bits{13};
 
 int plan_fused(int n, const std::vector<int>& q2s, const std::vector<PartLocal>& parts,
                int precision, std::vector<FusedPass>* out) {

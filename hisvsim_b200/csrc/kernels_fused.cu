@@ -716,30 +716,31 @@ __global__ void __launch_bounds__(kWsThreads, 1)
 // bounded by the producers' registers or per-thread load slots.  A raw
 // complex64 tile and its BF16 hi / lo B operand have the same size, so each
 // of the four buffers holds tile i first raw, then as B:
-//   warp 17     loader: for tile i, once the MMAs of tile i-4 have read
-//               buffer i%4 (bfree), arm rfull(i%4) with the tile's byte count
+//   warp 17     loader: for tile i, once the MMAs of tile i-NB have read
+//               buffer i%NB (bfree), arm rfull(i%NB) with the tile's byte count
 //               and copy the tile's contiguous runs (the lowest run of tile
 //               bits, slots 0..L0-1) in tile-index order;
-//   warps 0-7   producers: wait rfull(i%4), read their raw amplitudes into
+//   warps 0-7   producers: wait rfull(i%NB), read their raw amplitudes into
 //               registers, meet at a named barrier (every raw read precedes
 //               every B write), write the BF16 hi / lo rows, arrive on
-//               bfull(i%4);
-//   warp 16     MMA issue (commits to mdone(i%2) and bfree(i%4));
+//               bfull(i%NB);
+//   warp 16     MMA issue (commits to mdone(i%2) and bfree(i%NB));
 //   warps 8-15  epilogue: TMEM -> registers -> a per-warp shared-memory
 //               transpose -> 16-byte stores, each lane writing two amplitudes
 //               that are adjacent in memory, the lanes of a store covering
 //               contiguous runs.
-// Three tiles are in flight while one is converted.  Tiles up to 2^12
-// amplitudes.
+// With tiles of 2^12 amplitudes the ring has four buffers (three tiles in
+// flight while one is converted); tiles of 2^13 (contiguous runs twice as
+// long) fit two.
 constexpr int kBulkThreads = 576;  // 8 producer, 8 epilogue, 1 MMA, 1 loader warps
-constexpr int kBulkItems = 4;      // B items per producer thread (N * 16 / 256, N <= 64)
-constexpr int kBulkBuffers = 4;
+constexpr int kBulkItems = 8;      // B items per producer thread (N * 16 / 256, N <= 128)
+constexpr int kBulkBuffers = 4;    // ring buffers at most (2^(lgb) used)
 constexpr int kBulkMaxChunkBits = 9;  // bulk copies of at most 2^9 amplitudes (4 KiB)
 constexpr int kBulkStageFloats = 512;  // per epilogue warp: 16 p x 16 columns x (re, im)
 
 __global__ void __launch_bounds__(kBulkThreads, 1)
     k4_bulk(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
-            const uint8_t* __restrict__ a_all, int* __restrict__ err, int chunk_bits) {
+            const uint8_t* __restrict__ a_all, int* __restrict__ err, int chunk_bits, int lgb) {
   extern __shared__ __align__(1024) uint8_t sm[];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int m = P.m, T = 1 << m;
@@ -749,9 +750,10 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
   const uint32_t bbytes = uint32_t(N) * 256u;
   const int nchunks = T >> chunk_bits;
   const uint32_t chunk_bytes = 8u << chunk_bits;
+  const uint64_t bmask = (1u << lgb) - 1u;  // ring buffer of tile i: i & bmask
   uint8_t* sA = sm;
   uint8_t* sB = sA + kFusedABytes;  // [kBulkBuffers][T * 8 bytes]: raw tile, then hi | lo
-  uint64_t* gp = reinterpret_cast<uint64_t*>(sB + kBulkBuffers * size_t(T) * 8);
+  uint64_t* gp = reinterpret_cast<uint64_t*>(sB + (size_t(T) * 8 << lgb));
   uint64_t* gn = gp + 64;
   uint64_t* gc = gn + N;                                     // global offset of chunk c
   uint32_t* tq = reinterpret_cast<uint32_t*>(gc + nchunks);  // tile index of part index p
@@ -821,9 +823,8 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     // ---- loader
     uint64_t issued = 0;
     for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
-      const int b = int(i % kBulkBuffers);
-      if (i >= kBulkBuffers &&
-          !tc::mbar_wait(&bfree[b], uint32_t(i / kBulkBuffers - 1) & 1u, kWaitLimit)) {
+      const int b = int(i & bmask);
+      if ((i >> lgb) > 0 && !tc::mbar_wait(&bfree[b], uint32_t((i >> lgb) - 1) & 1u, kWaitLimit)) {
         fail();
         break;
       }
@@ -837,33 +838,29 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     }
     // no copy may still be landing when the CTA leaves: wait for the last
     // tile of each buffer (its phase is that buffer's latest)
-    for (uint64_t j = issued > kBulkBuffers ? issued - kBulkBuffers : 0; j < issued; ++j)
-      tc::mbar_wait(&rfull[j % kBulkBuffers], uint32_t(j / kBulkBuffers) & 1u, kWaitLimit);
+    for (uint64_t j = issued > bmask + 1 ? issued - bmask - 1 : 0; j < issued; ++j)
+      tc::mbar_wait(&rfull[j & bmask], uint32_t(j >> lgb) & 1u, kWaitLimit);
   } else if (warp < 8) {
     // ---- producers: item k is amplitudes p = 4kb..4kb+3 of column nn
-    const int nitems = (N * 16) / kWsProducers;  // 1..4
-    uint32_t roff[kBulkItems][4];  // byte offsets in the raw tile
-    uint32_t boff[kBulkItems];     // byte offset of the item's B row
-#pragma unroll
-    for (int k = 0; k < kBulkItems; ++k) {
-      const int item = (t + k * kWsProducers) & ((N * 16) - 1);
-      const int kb = item >> lgN, nn = item & (N - 1);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) roff[k][q] = (tq[4 * kb + q] | tn[nn]) * 8u;
-      boff[k] = tc::kmajor_off(uint32_t(nn), uint32_t(kb * 8), bk);
-    }
+    const int nitems = (N * 16) / kWsProducers;  // 1..8
     for (uint64_t i = 0; i < cnt; ++i) {
-      const int b = int(i % kBulkBuffers);
+      const int b = int(i & bmask);
       const bool ok =
-          !*abort_flag && tc::mbar_wait(&rfull[b], uint32_t(i / kBulkBuffers) & 1u, kWaitLimit);
+          !*abort_flag && tc::mbar_wait(&rfull[b], uint32_t(i >> lgb) & 1u, kWaitLimit);
       if (!ok) fail();
       uint8_t* buf = sB + size_t(b) * T * 8;
       float2 x[kBulkItems][4];
 #pragma unroll
       for (int k = 0; k < kBulkItems; ++k) {
         if (k >= nitems) break;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) x[k][q] = *reinterpret_cast<const float2*>(buf + roff[k][q]);
+        const int item = t + k * kWsProducers;
+        const int kb = item >> lgN, nn = item & (N - 1);
+        const uint32_t tcol = tn[nn];
+        const uint4 tp = *reinterpret_cast<const uint4*>(tq + 4 * kb);  // p = 4kb..4kb+3
+        x[k][0] = *reinterpret_cast<const float2*>(buf + size_t(tp.x | tcol) * 8);
+        x[k][1] = *reinterpret_cast<const float2*>(buf + size_t(tp.y | tcol) * 8);
+        x[k][2] = *reinterpret_cast<const float2*>(buf + size_t(tp.z | tcol) * 8);
+        x[k][3] = *reinterpret_cast<const float2*>(buf + size_t(tp.w | tcol) * 8);
       }
       // every raw read precedes every B write; the producers leave together
       // (a vote at the same named barrier) when any of them saw a timeout or
@@ -889,8 +886,10 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
           hw[q] = *reinterpret_cast<const uint32_t*>(&h);
           lw[q] = *reinterpret_cast<const uint32_t*>(&l);
         }
-        *reinterpret_cast<uint4*>(buf + boff[k]) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-        *reinterpret_cast<uint4*>(bl + boff[k]) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        const int item = t + k * kWsProducers;
+        const uint32_t boff = tc::kmajor_off(uint32_t(item & (N - 1)), uint32_t((item >> lgN) * 8), bk);
+        *reinterpret_cast<uint4*>(buf + boff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(bl + boff) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
       }
       tc::fence_proxy_async_smem();  // the B writes become visible to the tensor cores
       mbar_arrive(&bfull[b]);
@@ -957,8 +956,8 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     uint64_t issued = 0;
     for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
       const int b = int(i & 1);
-      const int bb = int(i % kBulkBuffers);
-      if (!tc::mbar_wait(&bfull[bb], uint32_t(i / kBulkBuffers) & 1u, kWaitLimit) ||
+      const int bb = int(i & bmask);
+      if (!tc::mbar_wait(&bfull[bb], uint32_t(i >> lgb) & 1u, kWaitLimit) ||
           (i >= 2 && !tc::mbar_wait(&tfree[b], uint32_t((i - 2) >> 1) & 1u, kWaitLimit))) {
         fail();
         break;
@@ -978,7 +977,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
         }
       }
       tc::mma_commit(&mdone[b]);
-      tc::mma_commit(&bfree[bb]);  // buffer bb may take tile i+4
+      tc::mma_commit(&bfree[bb]);  // buffer bb may take tile i + NB
       issued = i + 1;
     }
     // the last committed MMAs complete before TMEM is released
@@ -1032,7 +1031,7 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
   // the bulk form copies the lowest run of tile bits (slot 0 upward) and
   // stores two memory-adjacent amplitudes per lane: slot 0 must be tile bit
   // 0 and, when it belongs to the part, its local bit 0
-  bool bulk = P.nops == 1 && variant == 2 && P.m <= 12 && P.tile.n > 0 && P.tile.src[0] == 0 &&
+  bool bulk = P.nops == 1 && variant == 2 && P.m <= 13 && P.tile.n > 0 && P.tile.src[0] == 0 &&
               P.tile.dst[0] == 0 && P.tile.len[0] >= 2;
   for (int j = 1; j < kFusedBits; ++j) bulk = bulk && P.pbits[0][j] != 0;
   if (bulk) {
@@ -1045,16 +1044,18 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     }
     const int chunk_bits = std::min<int>(P.tile.len[0], kBulkMaxChunkBits);
     const int nchunks = T >> chunk_bits;
-    const size_t bsmem = size_t(kFusedABytes) + size_t(T) * 8 * kBulkBuffers + 64 * 8 +
-                         size_t(N) * 8 + size_t(nchunks) * 8 + 64 * 4 + size_t(N) * 4 +
-                         20 * 8 + 8 * kBulkStageFloats * 4;
+    const int lgb = P.m <= 12 ? 2 : 1;  // ring of four buffers, or two for 2^13 tiles
+    const size_t bsmem = size_t(kFusedABytes) + (size_t(T) * 8 << lgb) + 64 * 8 + size_t(N) * 8 +
+                         size_t(nchunks) * 8 + 64 * 4 + size_t(N) * 4 + 20 * 8 +
+                         8 * kBulkStageFloats * 4;
     if (bsmem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 bulk pass needs %zu B", bsmem);
     int bsms = 148, bdev = 0;
     HS_CUDA(cudaGetDevice(&bdev));
     HS_CUDA(cudaDeviceGetAttribute(&bsms, cudaDevAttrMultiProcessorCount, bdev));
     const int bgrid = int(P.ntiles < uint64_t(bsms) ? P.ntiles : uint64_t(bsms));
     k4_bulk<<<bgrid, kBulkThreads, bsmem, s>>>(static_cast<float2*>(amp), P,
-                                               static_cast<const uint8_t*>(d_a), d_err, chunk_bits);
+                                               static_cast<const uint8_t*>(d_a), d_err, chunk_bits,
+                                               lgb);
     HS_CUDA(cudaGetLastError());
     return HS_OK;
   }

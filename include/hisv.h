@@ -207,16 +207,16 @@ int hs_fused_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_o
 int hs_fused_apply(hs_state* st, const double* u, const int32_t* qubits, int precision,
                    void* stream);
 /* K4 kernel for one unitary per pass: 2 = bulk-loaded (default: a loader
- * warp streams tiles of up to 2^12 amplitudes into a four-deep shared-memory
- * ring with bulk copies, producer, MMA and epilogue warps hand tiles over
- * through mbarriers; passes that do not fit its shape run variant 1), 1 =
- * warp-specialised (producers load tiles of up to 2^13 straight from HBM), 0
- * = direct (CTA-wide barriers between load / MMA / drain).  Returns the
- * previous choice. */
+ * warp streams tiles into a shared-memory ring with bulk copies, four deep
+ * for tiles of up to 2^12 amplitudes, two deep for 2^13; producer, MMA and
+ * epilogue warps hand tiles over through mbarriers; passes that do not fit
+ * its shape run variant 1), 1 = warp-specialised (producers load tiles
+ * straight from HBM), 0 = direct (CTA-wide barriers between load / MMA /
+ * drain).  Returns the previous choice. */
 int hs_set_k4_variant(int variant);
 /* Shape of the fused passes: unitaries applied per state pass and tile bits,
- * 1 with 10..13 (default 1, 12: the bulk-loaded kernel's largest tile) or 2
- * with 10..12.  Returns the previous shape as ops * 100 + bits. */
+ * 1 with 10..13 (default 1, 13) or 2 with 10..12.  Returns the previous
+ * shape as ops * 100 + bits. */
 int hs_set_fused_shape(int max_ops_per_pass, int tile_bits);
 int hs_fused_compose(int num_qubits, const hs_gate* gates, const int32_t* part_offsets,
                      int num_parts, double* out_u, int32_t* out_qubits);

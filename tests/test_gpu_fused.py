@@ -125,10 +125,10 @@ def test_fused_pass_shapes(port, shape):
     assert np.abs(got - want).max() <= 1e-5
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant,bits", [(1, 13), (2, 12), (2, 13)])
 @pytest.mark.parametrize("qubits", [[11, 0, 5, 3, 9, 7], [0, 11, 5, 3, 9, 7], [12, 2, 5, 3, 9, 7],
                                     [1, 2, 3, 4, 5, 6]])
-def test_fused_apply_given_unitary(variant, qubits):
+def test_fused_apply_given_unitary(variant, bits, qubits):
     """hs_fused_apply with a random 64x64 unitary on scattered qubits, against
     numpy on the complex128 amplitudes: slot 0 as a later local bit (the
     bulk-loaded kernel hands such passes to the warp-specialised one), as
@@ -138,7 +138,7 @@ def test_fused_apply_given_unitary(variant, qubits):
     z = rng.normal(size=(64, 64)) + 1j * rng.normal(size=(64, 64))
     u, _ = np.linalg.qr(z)
     prev = abi.set_k4_variant(variant)
-    shape = abi.set_fused_shape(1, 12)  # the bulk-loaded kernel takes tiles up to 2^12
+    shape = abi.set_fused_shape(1, bits)
     try:
         _apply_and_check(n, u, qubits)
     finally:
@@ -164,7 +164,8 @@ def _apply_and_check(n, u, qubits):
     assert np.abs(got - want).max() <= 1e-5
 
 
-@pytest.mark.parametrize("variant,bits", [(0, 13), (1, 13), (1, 12), (2, 10), (2, 11), (2, 12)])
+@pytest.mark.parametrize("variant,bits", [(0, 13), (1, 13), (1, 12), (2, 10), (2, 11), (2, 12),
+                                          (2, 13)])
 @pytest.mark.parametrize("n", [10, 13, 17])
 def test_k4_variants(port, variant, bits, n):
     """The one-unitary-per-pass kernels (direct, warp-specialised,
