@@ -72,66 +72,154 @@ void runs(const std::vector<int>& dst, Runs* r) {
 }
 
 // Passes of one round for n qubits with tiles of at most `cap` bits: pass 0
-// takes qubits [0, cap) and the cost phase; later passes keep slots 0..2 for
-// contiguity and mix the next cap-3 qubits.
-int plan_passes(int n, int cap, int low, BatchInstance* I) {
-  std::vector<std::vector<int>> tiles, targets;
+// takes qubits [0, cap) (its RX targets); later passes keep the `low` lowest
+// qubits for contiguity and mix the next cap-low qubits.
+void round_passes(int n, int cap, int low, std::vector<std::vector<int>>* tiles,
+                  std::vector<std::vector<int>>* targets) {
+  tiles->clear();
+  targets->clear();
   if (n <= cap) {
     std::vector<int> all;
     for (int q = 0; q < n; ++q) all.push_back(q);
-    tiles.push_back(all);
-    targets.push_back(all);
+    tiles->push_back(all);
+    targets->push_back(all);
+    return;
+  }
+  std::vector<int> t0;
+  for (int q = 0; q < cap; ++q) t0.push_back(q);
+  tiles->push_back(t0);
+  targets->push_back(t0);
+  int covered = cap;
+  while (covered < n) {
+    const int nw = std::min(cap - low, n - covered);
+    std::vector<int> tl, tg;
+    for (int q = 0; q < low; ++q) tl.push_back(q);
+    for (int q = covered; q < covered + nw; ++q) {
+      tl.push_back(q);
+      tg.push_back(q);
+    }
+    // widen the tile with the next-lowest qubits (no gate on them in this
+    // pass): fewer, larger tiles and longer contiguous runs
+    for (int q = low; q < n && int(tl.size()) < cap; ++q)
+      if (std::find(tl.begin(), tl.end(), q) == tl.end()) tl.push_back(q);
+    std::sort(tl.begin(), tl.end());
+    tiles->push_back(tl);
+    targets->push_back(tg);
+    covered += nw;
+  }
+}
+
+// cut of the edges with both ends in the tile, for every tile index x < 2^m
+// (tile bit b is qubit tl[b])
+void cut_table(const std::vector<std::pair<int, int>>& edges, const std::vector<int>& tl,
+               uint8_t* out) {
+  std::vector<std::pair<int, int>> in;
+  auto bit_of = [&](int q) { return int(std::find(tl.begin(), tl.end(), q) - tl.begin()); };
+  for (const auto& e : edges) {
+    const int a = bit_of(e.first), b = bit_of(e.second);
+    if (a < int(tl.size()) && b < int(tl.size())) in.push_back({a, b});
+  }
+  for (uint32_t x = 0; x < (1u << tl.size()); ++x) {
+    int c = 0;
+    for (const auto& e : in) c += int(((x >> e.first) ^ (x >> e.second)) & 1u);
+    out[x] = uint8_t(c);
+  }
+}
+
+// kinds of pass: the first of the circuit (phase, then RX of its round), a
+// plain mixer pass, and a pass that ends one round and starts the next
+enum StepKind { kFirst, kMix, kJoin };
+
+// All steps of an instance: p rounds of the round's passes.  Round r+1 runs
+// the passes in the opposite order of round r, so the pass that ends round
+// r is also the one that starts round r+1, and the two share one state pass
+// (RX of round r, cost phase and RX of round r+1 in one visit of the tile):
+// np + (p-1)(np-1) steps instead of p np.  With a single pass per round every
+// step is phase + RX of its round.
+int plan_steps(int n, int cap, int low, int p, const std::vector<std::pair<int, int>>& edges,
+               BatchInstance* I, std::vector<uint8_t>* cut) {
+  std::vector<std::vector<int>> tiles, targets;
+  round_passes(n, cap, low, &tiles, &targets);
+  const int np = int(tiles.size());
+  if (np > kBatchMaxPasses)
+    return set_error(HS_E_UNSUPPORTED, "%d qubits need %d passes with %d-qubit tiles (max %d)", n, np,
+                     cap, kBatchMaxPasses);
+  struct Step {
+    int pass, kind, ra, rb;
+  };
+  std::vector<Step> steps;
+  if (np == 1) {
+    for (int r = 0; r < p; ++r) steps.push_back({0, kFirst, r, r});
   } else {
-    std::vector<int> t0;
-    for (int q = 0; q < cap; ++q) t0.push_back(q);
-    tiles.push_back(t0);
-    targets.push_back(t0);
-    int covered = cap;
-    while (covered < n) {
-      const int nw = std::min(cap - low, n - covered);
-      std::vector<int> tl, tg;
-      for (int q = 0; q < low; ++q) tl.push_back(q);
-      for (int q = covered; q < covered + nw; ++q) {
-        tl.push_back(q);
-        tg.push_back(q);
+    std::vector<int> order(np);
+    for (int j = 0; j < np; ++j) order[j] = j;
+    steps.push_back({order[0], kFirst, 0, 0});
+    for (int r = 0; r < p; ++r) {
+      for (int j = 1; j < np - 1; ++j) steps.push_back({order[j], kMix, r, r});
+      if (r + 1 < p) {
+        steps.push_back({order[np - 1], kJoin, r, r + 1});
+        std::reverse(order.begin(), order.end());
+      } else {
+        steps.push_back({order[np - 1], kMix, r, r});
       }
-      // widen the tile with the next-lowest qubits (no gate on them in this
-      // pass): fewer, larger tiles and longer contiguous runs
-      for (int q = low; q < n && int(tl.size()) < cap; ++q)
-        if (std::find(tl.begin(), tl.end(), q) == tl.end()) tl.push_back(q);
-      std::sort(tl.begin(), tl.end());
-      tiles.push_back(tl);
-      targets.push_back(tg);
-      covered += nw;
     }
   }
-  if (int(tiles.size()) > kBatchMaxPasses)
-    return set_error(HS_E_UNSUPPORTED, "%d qubits need %d passes with %d-qubit tiles (max %d)", n,
-                     int(tiles.size()), cap, kBatchMaxPasses);
-  I->npasses = int(tiles.size());
-  for (int j = 0; j < I->npasses; ++j) {
-    BatchPass& P = I->pass[j];
+  if (int(steps.size()) > kBatchMaxSteps)
+    return set_error(HS_E_UNSUPPORTED, "%d qubits x %d rounds need %d passes (max %d)", n, p,
+                     int(steps.size()), kBatchMaxSteps);
+  I->nsteps = int(steps.size());
+  cut->clear();
+  for (int k = 0; k < I->nsteps; ++k) {
+    const Step& st = steps[k];
+    BatchPass& P = I->pass[k];
     std::memset(&P, 0, sizeof(P));
-    const std::vector<int>& tl = tiles[j];
+    const std::vector<int>& tl = tiles[st.pass];
     P.m = int(tl.size());
     runs(tl, &P.tile);
     for (int b = 0; b < P.m; ++b) P.tile_slot[b] = uint8_t(tl[b]);
+    for (int q = 0; q < kBatchMaxQubits; ++q) P.tbit[q] = -1;
+    for (int b = 0; b < P.m; ++b) P.tbit[tl[b]] = int8_t(b);
     std::vector<int> outer;
     for (int q = 0; q < n; ++q)
       if (std::find(tl.begin(), tl.end(), q) == tl.end()) outer.push_back(q);
     runs(outer, &P.outer);
-    P.phase = j == 0;
     std::vector<int> tb;  // target tile bits
-    for (int q : targets[j]) tb.push_back(int(std::find(tl.begin(), tl.end(), q) - tl.begin()));
+    for (int q : targets[st.pass]) tb.push_back(int(std::find(tl.begin(), tl.end(), q) - tl.begin()));
     P.ngroups = int((tb.size() + 3) / 4);
+    uint8_t gmask[3] = {0, 0, 0};
     for (int g = 0; g < P.ngroups; ++g) {
       std::vector<int> regs;
       for (size_t x = 4 * g; x < tb.size() && regs.size() < 4; ++x) regs.push_back(tb[x]);
-      const int ntg = int(regs.size());
+      gmask[g] = uint8_t((1 << regs.size()) - 1);
       for (int b = P.m - 1; b >= 0 && regs.size() < 4; --b)
         if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
-      for (int k = 0; k < 4; ++k) P.group_bits[g][k] = uint8_t(regs[k]);
-      P.group_rx[g] = uint8_t((1 << ntg) - 1);
+      for (int j = 0; j < 4; ++j) P.group_bits[g][j] = uint8_t(regs[j]);
+    }
+    P.ra = uint8_t(st.ra);
+    P.rb = uint8_t(st.rb);
+    const int G = P.ngroups;
+    auto visit = [&](int g, uint8_t a, uint8_t ph, uint8_t b) {
+      const int v = P.nvisits++;
+      P.visit_group[v] = uint8_t(g);
+      P.rx_a[v] = a;
+      P.ph[v] = ph;
+      P.rx_b[v] = b;
+    };
+    if (st.kind == kFirst) {
+      for (int g = 0; g < G; ++g) visit(g, 0, g == 0, gmask[g]);
+    } else if (st.kind == kMix) {
+      for (int g = 0; g < G; ++g) visit(g, gmask[g], 0, 0);
+    } else {
+      for (int g = 0; g < G - 1; ++g) visit(g, gmask[g], 0, 0);
+      visit(G - 1, gmask[G - 1], 1, gmask[G - 1]);
+      for (int g = G - 2; g >= 0; --g) visit(g, 0, 0, gmask[g]);
+    }
+    P.phase = st.kind != kMix;
+    if (P.phase) {
+      cut->resize((cut->size() + 15) & ~size_t(15));  // 16-byte aligned tables
+      P.cut_off = uint32_t(cut->size());
+      cut->resize(cut->size() + (size_t(1) << P.m));
+      cut_table(edges, tl, cut->data() + P.cut_off);
     }
   }
   return HS_OK;
@@ -157,18 +245,6 @@ int upload_params(hs_batch* b) {
   return HS_OK;
 }
 
-// cut of the edges with both ends in qubits [0, m), for every x < 2^m
-void cut_low_table(const std::vector<std::pair<int, int>>& edges, int m, uint8_t* out) {
-  std::vector<std::pair<int, int>> in;
-  for (const auto& e : edges)
-    if (e.first < m && e.second < m) in.push_back(e);
-  for (uint32_t x = 0; x < (1u << m); ++x) {
-    int c = 0;
-    for (const auto& e : in) c += int(((x >> e.first) ^ (x >> e.second)) & 1u);
-    out[x] = uint8_t(c);
-  }
-}
-
 int build_plan(hs_batch* b) {
   free_plan(b);
   std::vector<BatchInstance> inst(b->ninst);
@@ -177,7 +253,7 @@ int build_plan(hs_batch* b) {
   int maxsteps = 0;
   b->pass_bytes = 0;
   std::vector<size_t> cut_off(b->ninst);
-  size_t cut_bytes = 0;
+  std::vector<uint8_t> cut, icut;
   int max_m = 0;
   for (int i = 0; i < b->ninst; ++i) {
     BatchInstance& I = inst[i];
@@ -189,23 +265,23 @@ int build_plan(hs_batch* b) {
       I.edge_a[e] = uint8_t(b->edges[i][e].first);
       I.edge_b[e] = uint8_t(b->edges[i][e].second);
     }
-    HS_TRY(plan_passes(I.n, b->cap_of_n[I.n] ? b->cap_of_n[I.n] : b->tile_cap, b->low_keep, &I));
-    for (int j = 0; j < I.npasses; ++j) max_m = std::max(max_m, int(I.pass[j].m));
+    HS_TRY(plan_steps(I.n, b->cap_of_n[I.n] ? b->cap_of_n[I.n] : b->tile_cap, b->low_keep, b->p,
+                      b->edges[i], &I, &icut));
+    for (int j = 0; j < I.nsteps; ++j) max_m = std::max(max_m, int(I.pass[j].m));
     I.step_base = nc;
-    const int steps = I.npasses * b->p;
+    const int steps = I.nsteps;
     nc += uint64_t(steps);
     maxsteps = std::max(maxsteps, steps);
     for (int k = 0; k < steps; ++k) b->pass_bytes += 2ull * (8ull << I.n);
-    cut_off[i] = cut_bytes;
-    cut_bytes += size_t(1) << I.pass[0].m;
+    // 16-byte aligned tables (the kernel stages them with 16-byte loads)
+    cut_off[i] = cut.size();
+    cut.insert(cut.end(), icut.begin(), icut.end());
+    cut.resize((cut.size() + 15) & ~size_t(15));
   }
   b->threads = max_m > 11 ? 256 : 128;
-  std::vector<uint8_t> cut(cut_bytes);
-  for (int i = 0; i < b->ninst; ++i)
-    cut_low_table(b->edges[i], inst[i].pass[0].m, cut.data() + cut_off[i]);
-  HS_CUDA(cudaMalloc(&b->d_cut, cut_bytes));
-  HS_CUDA(cudaMemcpy(b->d_cut, cut.data(), cut_bytes, cudaMemcpyHostToDevice));
-  for (int i = 0; i < b->ninst; ++i) inst[i].cut_low = b->d_cut + cut_off[i];
+  HS_CUDA(cudaMalloc(&b->d_cut, cut.size()));
+  HS_CUDA(cudaMemcpy(b->d_cut, cut.data(), cut.size(), cudaMemcpyHostToDevice));
+  for (int i = 0; i < b->ninst; ++i) inst[i].cut = b->d_cut + cut_off[i];
   // work items: per step level, per instance, the step's tiles in chunks
   std::vector<BatchItem> items;
   std::vector<uint32_t> prev_chunks(b->ninst, 0);
@@ -213,12 +289,12 @@ int build_plan(hs_batch* b) {
   for (int k = 0; k < maxsteps; ++k)
     for (int i = 0; i < b->ninst; ++i) {
       const BatchInstance& I = inst[i];
-      if (k >= I.npasses * b->p) continue;
+      if (k >= I.nsteps) continue;
       BatchItem it;
       it.first = total;
       it.inst = i;
       it.step = k;
-      it.ntiles = uint32_t(1ull << (I.n - I.pass[k % I.npasses].m));
+      it.ntiles = uint32_t(1ull << (I.n - I.pass[k].m));
       it.chunk = std::min<uint32_t>(uint32_t(b->chunk), it.ntiles);
       it.need = prev_chunks[i];
       const uint32_t nchunks = (it.ntiles + it.chunk - 1) / it.chunk;

@@ -187,29 +187,46 @@ constexpr int kBatchMaxQubits = 30;
 constexpr int kBatchMaxEdges = 64;
 constexpr int kBatchMaxRounds = 8;
 constexpr int kBatchMaxPasses = 4;   // passes per round
+constexpr int kBatchMaxSteps = 32;   // passes over an instance's state, all rounds
+constexpr int kBatchMaxVisits = 5;   // register-group visits per pass
 // 16 amplitudes per thread: CTAs of 128 threads take tiles of up to 2^11,
 // CTAs of 256 threads tiles of up to 2^12
 constexpr int kBatchMaxTileBits = 12;
 
-// one pass of a QAOA round over an instance: the tile bits, which of them get
-// the mixer RX, in register groups of 4 (tile-bit positions)
+// one pass over an instance's state: the tile bits, register groups of 4
+// tile bits, and the group visits in order.  A visit loads its group's
+// amplitudes into registers, applies RX of round ra to the register bits in
+// rx_a, then (ph) the cost phase of round rb, then RX of round rb to the bits
+// in rx_b.  A pass that ends round r and starts round r+1 visits its groups
+// forward with round r's RX, applies the phase in the last group, and visits
+// them backward with round r+1's RX.
 struct BatchPass {
   int32_t m;                 // tile bits
-  int32_t ngroups;
+  int32_t ngroups;           // register groups (<= 3)
+  int32_t nvisits;           // group visits (<= kBatchMaxVisits)
+  uint32_t cut_off;          // byte offset of this pass's cut table (phase passes)
   Runs tile, outer;
   uint8_t tile_slot[16];
   uint8_t group_bits[3][4];  // tile bits in registers per group (4 each)
-  uint8_t group_rx[3];       // bit j set: register bit j of the group gets RX
-  uint8_t phase;             // 1: the cost phase is applied in group 0
+  uint8_t visit_group[kBatchMaxVisits];
+  uint8_t rx_a[kBatchMaxVisits];  // bit j set: register bit j gets RX of round ra
+  uint8_t ph[kBatchMaxVisits];    // 1: then the cost phase of round rb
+  uint8_t rx_b[kBatchMaxVisits];  // bit j set: then RX of round rb
+  uint8_t ra, rb;
+  uint8_t phase;             // 1: a visit applies the cost phase
+  int8_t tbit[kBatchMaxQubits];   // tile bit of qubit q, -1 outside the tile
+  uint8_t pad[5];
 };
 
 struct BatchInstance {
   float2* amp;
-  int32_t n, nedges, p, npasses;
+  int32_t n, nedges, p, nsteps;
   uint8_t edge_a[kBatchMaxEdges], edge_b[kBatchMaxEdges];
-  BatchPass pass[kBatchMaxPasses];
+  BatchPass pass[kBatchMaxSteps];
   uint64_t step_base;        // index of this instance's first counter
-  const uint8_t* cut_low;    // 2^pass[0].m entries: cut of the edges inside qubits [0, m)
+  // cut tables of the phase passes (2^m entries each: cut of the edges with
+  // both ends in the pass's tile); pass 0's comes first (tile = qubits [0, m))
+  const uint8_t* cut;
 };
 
 struct BatchParams {         // per instance per round (updated for sweeps)

@@ -1,8 +1,11 @@
 // K6: the batching form.  Many QAOA MaxCut instances of different qubit counts
 // are advanced by ONE persistent launch.  A step of an instance is one pass
-// over its complex64 state: the first pass of a round applies the cost phase
-// e^{i gamma/2 (2 cut(x) - |E|)} = prod_E RZZ(gamma), every pass applies the
-// mixer RX(2 beta) to its share of the qubits.  The tiles of a step are cut
+// over its complex64 state: a pass applies the mixer RX(2 beta) to its share
+// of the qubits, and the pass that ends round r also applies the cost phase
+// e^{i gamma/2 (2 cut(x) - |E|)} = prod_E RZZ(gamma) of round r+1 and round
+// r+1's RX on the same qubits (the rounds run their passes in alternating
+// order, so the pass that ends one round starts the next; the planner's
+// descriptors say what each register-group visit applies).  The tiles of a step are cut
 // into chunks; CTAs take chunks from a global queue in step order and stream
 // their tiles through two shared-memory buffers (the next tile loads while
 // the current one is processed).  A chunk of step k waits until every chunk
@@ -10,11 +13,11 @@
 // dequeued in step order, so the earliest unfinished chunk never waits and
 // the queue always drains.  Waits are bounded: a timeout sets an error flag.
 //
-// cut(x) in the phase pass: the tile holds qubits [0, m), so with the outer
-// bits fixed, cut(x) = cut_low[i] + C + sum_q w_q i_q, where cut_low counts
-// the edges inside [0, m) (a per-instance table), C the edges outside it plus
-// the crossing edges whose outer end is 1, and w_q = (#crossing edges of q
-// whose outer end is 0) - (#those whose outer end is 1).
+// cut(x) in a phase pass: with the outer bits fixed, cut(x) = cut_table[i] +
+// C + sum_b w_b i_b over the tile bits b, where cut_table counts the edges
+// with both ends in the tile (a table per phase pass), C the edges outside it
+// plus the crossing edges whose outer end is 1, and w_b = (#crossing edges
+// at tile bit b whose outer end is 0) - (#those whose outer end is 1).
 #include "internal.h"
 
 namespace hisv {
@@ -51,6 +54,7 @@ struct Shared {
   uint8_t ea[kBatchMaxEdges], eb[kBatchMaxEdges];
   uint64_t gk[8];  // global offset of chunk k * NT
   uint32_t gro[4];  // last group: global offset of each register bit
+  float2 rx[2];     // (cos beta, sin beta) of rounds ra and rb
   int w[2][16];  // per tile buffer: warp 0 prepares the next tile's weights
   int c[2];      // while the other warps may still read the current ones
   int group;
@@ -58,9 +62,13 @@ struct Shared {
   unsigned long long item;
 };
 
-// w_q and C of the tile whose outer bits are gbase (warp 0 only)
+// (C, w) of the tile whose outer bits are gbase (warp 0 only): tbit[q] is the
+// tile bit of qubit q or -1; an edge with one end in the tile at bit b adds
+// i_b (outer end 0) or 1 - i_b (outer end 1), one with both ends outside adds
+// its fixed value, and edges inside the tile are in the pass's cut table
 template <class Sh>
-__device__ __forceinline__ void cross_weights(Sh& S, int nedges, int m, uint64_t gbase, int buf) {
+__device__ __forceinline__ void cross_weights(Sh& S, int nedges, const int8_t* tbit, uint64_t gbase,
+                                              int buf) {
   const int lane = threadIdx.x & 31;
   int* w = S.w[buf];
   if (lane < 16) w[lane] = 0;
@@ -68,16 +76,16 @@ __device__ __forceinline__ void cross_weights(Sh& S, int nedges, int m, uint64_t
   int c = 0;
   for (int e = lane; e < nedges; e += 32) {
     const int a = S.ea[e], b = S.eb[e];
+    const int ta = tbit[a], tb = tbit[b];
     const int xa = int((gbase >> a) & 1ull), xb = int((gbase >> b) & 1ull);
-    const bool la = a < m, lb = b < m;
-    if (!la && !lb) {
+    if (ta < 0 && tb < 0) {
       c += xa ^ xb;
-    } else if (la && !lb) {
+    } else if (ta >= 0 && tb < 0) {
       c += xb;
-      atomicAdd(&w[a], xb ? -1 : 1);
-    } else if (!la && lb) {
+      atomicAdd(&w[ta], xb ? -1 : 1);
+    } else if (ta < 0 && tb >= 0) {
       c += xa;
-      atomicAdd(&w[b], xa ? -1 : 1);
+      atomicAdd(&w[tb], xa ? -1 : 1);
     }
   }
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -132,32 +140,34 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
     const BatchItem G = groups[S.group];
     const BatchInstance& I = insts[G.inst];
     const int k = G.step;
-    const int round = k / I.npasses, pj = k - round * I.npasses;
     {
       // the pass descriptor is read many times per tile: keep it in shared memory
       static_assert(sizeof(BatchPass) % 4 == 0, "BatchPass words");
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(&I.pass[pj]);
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&I.pass[k]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&S.pass);
       for (int w = t; w < int(sizeof(BatchPass) / 4); w += kBatchThreads) dst[w] = src[w];
     }
     __syncthreads();
     const BatchPass& P = S.pass;
-    const int m = P.m, T = 1 << m, ngr = P.ngroups, nedges = I.nedges;
+    const int m = P.m, T = 1 << m, ngr = P.ngroups, nv = P.nvisits, nedges = I.nedges;
     const bool phase = P.phase != 0;
     const uint32_t t_begin = uint32_t(item - G.first) * G.chunk;
     const uint32_t t_end = min(G.ntiles, t_begin + G.chunk);
     float2* amp = I.amp;
     if (phase) {
-      if (t < nedges + 1) S.phase[t] = pars[G.inst].phase[round][t];
+      if (t < nedges + 1) S.phase[t] = pars[G.inst].phase[P.rb][t];
       if (t < nedges) {
         S.ea[t] = I.edge_a[t];
         S.eb[t] = I.edge_b[t];
       }
-      const uint4* cs = reinterpret_cast<const uint4*>(I.cut_low);
+      const uint4* cs = reinterpret_cast<const uint4*>(I.cut + P.cut_off);
       uint4* cd = reinterpret_cast<uint4*>(S.cut);
-      for (int i = t; i < T / 16; i += kBatchThreads) cd[i] = cs[i];
+      for (int i = t; i < (T + 15) / 16; i += kBatchThreads) cd[i] = cs[i];
     }
-    const float2 rx = pars[G.inst].rx[round][0];  // (cos beta, sin beta)
+    if (t == 0) {
+      S.rx[0] = pars[G.inst].rx[P.ra][0];  // (cos beta, sin beta) of round ra
+      S.rx[1] = pars[G.inst].rx[P.rb][0];  // and of round rb
+    }
     const bool active = t < (T >> 4);
     // 16-byte chunk c = t + k * threads covers tile indices 2c, 2c + 1; the
     // bits of t and of k * threads are disjoint, so its global offset is
@@ -168,23 +178,24 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
     // thread bits of each register group: the tile bits not held in registers;
     // bswz is linear over GF(2), so a register element's slot is
     // bswz(thread part) ^ (XOR of bswz(register bit))
-    uint32_t sbase[3] = {0, 0, 0}, thr0 = 0, thr_last = 0;
-    for (int g = 0; g < ngr; ++g) {
+    // (the thread part of group g, recomputed where the phase needs it)
+    auto thread_part = [&](int g) {
       uint32_t rmask = 0, thr = 0;
       for (int j = 0; j < 4; ++j) rmask |= 1u << P.group_bits[g][j];
       int src = 0;
       for (int b = 0; b < m; ++b)
         if (!((rmask >> b) & 1u)) thr |= uint32_t((t >> src++) & 1) << b;
-      sbase[g] = bswz(thr);
-      if (g == 0) thr0 = thr;
-      if (g == ngr - 1) thr_last = thr;
-    }
-    // the last group writes its registers straight to global memory: the
+      return thr;
+    };
+    uint32_t sbase[3] = {0, 0, 0};
+    for (int g = 0; g < ngr; ++g) sbase[g] = bswz(thread_part(g));
+    // the last visit writes its registers straight to global memory: the
     // thread part's offset and each register bit's offset (disjoint bits add)
     // (instances have at most 30 qubits, so offsets within a state fit 32 bits)
-    const uint32_t gl_base = uint32_t(bdep(thr_last, P.tile));
-    if (t < 4) S.gro[t] = uint32_t(bdep(1ull << P.group_bits[ngr - 1][t], P.tile));
-    __syncthreads();  // S.gk, S.gro
+    const int glast = P.visit_group[nv - 1];
+    const uint32_t gl_base = uint32_t(bdep(thread_part(glast), P.tile));
+    if (t < 4) S.gro[t] = uint32_t(bdep(1ull << P.group_bits[glast][t], P.tile));
+    __syncthreads();  // S.gk, S.gro, S.rx
     // prologue: first tile into buffer 0
     {
       const uint64_t gb = bdep(t_begin, P.outer) + gt;
@@ -197,9 +208,9 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
       float2* tile = tiles + buf * kTileMax;
       const uint64_t gbase = bdep(ti, P.outer);
       cp_wait<0>();  // this tile's copies (the only ones in flight)
-      if (phase && t < 32) cross_weights(S, nedges, m, gbase, buf);
+      if (phase && t < 32) cross_weights(S, nedges, P.tbit, gbase, buf);
       // one barrier per tile: every thread's copies and the weights are
-      // visible, and every thread is past the previous tile's last group,
+      // visible, and every thread is past the previous tile's last visit,
       // so the other buffer may be refilled
       __syncthreads();
       if (ti + 1 < t_end) {
@@ -209,7 +220,9 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
           cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nb + S.gk[k]);
         cp_commit();
       }
-      for (int g = 0; g < ngr; ++g) {
+      for (int vi = 0; vi < nv; ++vi) {
+        const int g = P.visit_group[vi];
+        const uint32_t sbg = sbase[g];
         if (active) {
           uint32_t so[4];
 #pragma unroll
@@ -217,42 +230,14 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
           float2 v[16];
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
-            uint32_t a = sbase[g];
+            uint32_t a = sbg;
 #pragma unroll
             for (int j = 0; j < 4; ++j)
               if ((e >> j) & 1) a ^= so[j];
             v[e] = tile[a];
           }
-          if (g == 0 && phase) {
-            // cut = cut_low[i] + C + sum_q w_q i_q (tile bit q is qubit q)
-            const int* wt = S.w[buf];
-            int dthr = S.c[buf];
-            for (int b = 0; b < m; ++b)
-              if ((thr0 >> b) & 1u) dthr += wt[b];
-            int wr[4];
-            uint32_t rb[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              wr[j] = wt[P.group_bits[0][j]];
-              rb[j] = 1u << P.group_bits[0][j];
-            }
-#pragma unroll
-            for (int e = 0; e < 16; ++e) {
-              uint32_t idx = thr0;
-              int cc = dthr;
-#pragma unroll
-              for (int j = 0; j < 4; ++j)
-                if ((e >> j) & 1) {
-                  idx |= rb[j];
-                  cc += wr[j];
-                }
-              const float2 ph = S.phase[int(S.cut[idx]) + cc];
-              const float2 a = v[e];
-              v[e] = make_float2(ph.x * a.x - ph.y * a.y, ph.x * a.y + ph.y * a.x);
-            }
-          }
-          // mixer RX(2 beta) = [[c, -i s], [-i s, c]] on the group's target bits
-          auto rx_bit = [&](int j) {
+          // mixer RX(2 beta) = [[c, -i s], [-i s, c]] on register bit j
+          auto rx_bit = [&](int j, float2 rx) {
 #pragma unroll
             for (int e0 = 0; e0 < 16; ++e0) {
               if ((e0 >> j) & 1) continue;
@@ -262,20 +247,57 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
               v[e1] = make_float2(rx.y * a.y + rx.x * b.x, -rx.y * a.x + rx.x * b.y);
             }
           };
-          const int gm = P.group_rx[g];
-          if (gm == 15) {  // the common case: all four register bits are targets
-            rx_bit(0);
-            rx_bit(1);
-            rx_bit(2);
-            rx_bit(3);
-          } else {
-            if (gm & 1) rx_bit(0);
-            if (gm & 2) rx_bit(1);
-            if (gm & 4) rx_bit(2);
-            if (gm & 8) rx_bit(3);
+          auto rx_mask = [&](int gm, float2 rx) {
+            if (gm == 15) {  // the common case: all four register bits are targets
+              rx_bit(0, rx);
+              rx_bit(1, rx);
+              rx_bit(2, rx);
+              rx_bit(3, rx);
+            } else {
+              if (gm & 1) rx_bit(0, rx);
+              if (gm & 2) rx_bit(1, rx);
+              if (gm & 4) rx_bit(2, rx);
+              if (gm & 8) rx_bit(3, rx);
+            }
+          };
+          // RX of round ra, then the cost phase and RX of round rb: one copy
+          // of the RX code for both
+#pragma unroll 1
+          for (int h = 0; h < 2; ++h) {
+            if (h == 1 && P.ph[vi]) {
+              // cut = cut_table[i] + C + sum_b w_b i_b over the tile bits b
+              const uint32_t thr = thread_part(g);
+              const int* wt = S.w[buf];
+              int dthr = S.c[buf];
+              for (int b = 0; b < m; ++b)
+                if ((thr >> b) & 1u) dthr += wt[b];
+              int wr[4];
+              uint32_t rb[4];
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                wr[j] = wt[P.group_bits[g][j]];
+                rb[j] = 1u << P.group_bits[g][j];
+              }
+#pragma unroll
+              for (int e = 0; e < 16; ++e) {
+                uint32_t idx = thr;
+                int cc = dthr;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                  if ((e >> j) & 1) {
+                    idx |= rb[j];
+                    cc += wr[j];
+                  }
+                const float2 ph = S.phase[int(S.cut[idx]) + cc];
+                const float2 a = v[e];
+                v[e] = make_float2(ph.x * a.x - ph.y * a.y, ph.x * a.y + ph.y * a.x);
+              }
+            }
+            const int gm = h ? P.rx_b[vi] : P.rx_a[vi];
+            if (gm) rx_mask(gm, S.rx[h]);
           }
-          if (g == ngr - 1) {
-            // last group: registers straight to global memory (the lanes run
+          if (vi == nv - 1) {
+            // last visit: registers straight to global memory (the lanes run
             // over the low, contiguous tile bits, so the stores coalesce)
             float2* base = amp + gbase + gl_base;
             uint32_t ro[4];
@@ -292,7 +314,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
           } else {
 #pragma unroll
             for (int e = 0; e < 16; ++e) {
-              uint32_t a = sbase[g];
+              uint32_t a = sbg;
 #pragma unroll
               for (int j = 0; j < 4; ++j)
                 if ((e >> j) & 1) a ^= so[j];
@@ -300,9 +322,9 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
             }
           }
         }
-        // the next group reads what this one wrote; after the last group the
+        // the next visit reads what this one wrote; after the last visit the
         // next tile's first barrier protects the buffer
-        if (g < ngr - 1) __syncthreads();
+        if (vi < nv - 1) __syncthreads();
       }
     }
     __threadfence();
@@ -327,7 +349,7 @@ __global__ void k6_init(const BatchInstance* __restrict__ insts) {
 }
 
 // <H_C> = sum_x |a_x|^2 cut(x) in FP64.  Block (b, instance) takes ranges of
-// 2^m amplitudes (m = the phase pass's tile bits, so cut_low applies) r = b,
+// 2^m amplitudes (m = the first phase pass's tile bits, so its cut table applies) r = b,
 // b + gridDim.x, ...; per range warp 0 derives C and w_q as in K6, then every
 // thread sums its amplitudes.  Per-block partials, added in order by
 // k6_expect_finish: the result does not depend on timing.
@@ -340,7 +362,9 @@ __global__ void __launch_bounds__(256) k6_expect(const BatchInstance* __restrict
   const BatchInstance& I = insts[blockIdx.y];
   const int m = I.pass[0].m, nedges = I.nedges, t = threadIdx.x;
   const uint64_t nranges = 1ull << (I.n - m);
-  for (int i = t; i < (1 << m); i += 256) S.cut[i] = I.cut_low[i];
+  // step 0 is the first phase pass: its tile is qubits [0, m), its cut table
+  // comes first
+  for (int i = t; i < (1 << m); i += 256) S.cut[i] = I.cut[I.pass[0].cut_off + i];
   if (t < nedges) {
     S.ea[t] = I.edge_a[t];
     S.eb[t] = I.edge_b[t];
@@ -348,7 +372,7 @@ __global__ void __launch_bounds__(256) k6_expect(const BatchInstance* __restrict
   double s = 0;
   for (uint64_t r = blockIdx.x; r < nranges; r += gridDim.x) {
     __syncthreads();
-    if (t < 32) cross_weights(S, nedges, m, r << m, 0);
+    if (t < 32) cross_weights(S, nedges, I.pass[0].tbit, r << m, 0);
     __syncthreads();
     const float2* a = I.amp + (r << m);
     for (int i = t; i < (1 << m); i += 256) {
