@@ -73,6 +73,7 @@ enum OpKind : uint8_t {
 //   2q dense, uncontrolled (v -> other array):      64 + pair        (64..69)
 //   2q dense, controlled (in place):                72 + pair        (72..77)
 //   2q swap (in place):                             80 + pair        (80..85)
+//   1q dense, uncontrolled, real top-left (in place): 88 + ja        (88..91)
 enum TargetWhere : uint8_t { TW_NONE = 0, TW_REG = 1, TW_THR = 2, TW_OUT = 3 };
 
 struct DevOp {

@@ -112,6 +112,28 @@ __device__ __forceinline__ void d1x(const V (&s)[1 << R], V (&d)[1 << R], const 
   }
 }
 
+// dense 2x2 with a real top-left coefficient on register bit J, in place
+template <int R, int J, typename V>
+__device__ __forceinline__ void d1r(V (&v)[1 << R], const double2* __restrict__ c) {
+  using T = typename Scalar<V>::T;
+  constexpr int E = 1 << R;
+  const T c0 = T(c[0].x), c1r = T(c[1].x), c1i = T(c[1].y);
+  const double2 c2 = c[2], c3 = c[3];
+#pragma unroll
+  for (int p = 0; p < E / 2; ++p) {
+    const int e0 = ins0<J>(p), e1 = e0 | (1 << J);
+    const V a = v[e0], b = v[e1];
+    T re = c0 * a.x;
+    re = fma(c1r, b.x, re);
+    re = fma(-c1i, b.y, re);
+    T im = c0 * a.y;
+    im = fma(c1r, b.y, im);
+    im = fma(c1i, b.x, im);
+    v[e0] = mk<V>(re, im);
+    v[e1] = cmac2(c2, a, c3, b);
+  }
+}
+
 // dense 2x2 on register bit J, in place, for pairs whose controls hold
 template <int R, int J, typename V>
 __device__ __forceinline__ void d1c(V (&v)[1 << R], const double2* __restrict__ c, uint32_t creg,
@@ -288,8 +310,11 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
   case (J): if constexpr ((J) < R) d1c<R, J>(v, c, 0u, true); break;
 #define D2(P, JA, JB) \
   case 64 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, 0u, true); break;
+#define DR(J) \
+  case 88 + (J): if constexpr ((J) < R) d1r<R, J>(v, c); break;
   switch (op.code) {
     D1(0) D1(1) D1(2) D1(3)
+    DR(0) DR(1) DR(2) DR(3)
     D2(0, 0, 1) D2(1, 0, 2) D2(2, 0, 3) D2(3, 1, 2) D2(4, 1, 3) D2(5, 2, 3)
     C1(0) C1(1) C1(2) C1(3)
     case 16:  // sign flip of every element of the thread (mask outside the registers)
@@ -307,6 +332,7 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
   }
 #undef D1
 #undef D2
+#undef DR
 #undef C1
 #undef NEG
 #undef PH
