@@ -387,6 +387,8 @@ __device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32
 // leaves room for three CTAs per SM (FP64-heavy passes need the extra warps
 // to hide latency; with two-qubit dense ops, R = 3 takes two CTAs of 256
 // threads so that the 4x4 bodies do not spill)
+constexpr int kThrCache = 4;  // groups whose thread parts are tabulated per launch
+
 template <typename V, int R, bool FULL>
 struct K1Threads {
   static constexpr int value = 256;
@@ -418,6 +420,9 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   // (after the chunk table; kept in shared memory to spare registers)
   uint64_t* s_glreg = s_gchunk + per_thr;
   uint64_t* s_glthr = s_glreg + R;
+  // the thread part (tile index bits held by this thread) of the first
+  // kThrCache groups, the same in every tile
+  uint32_t* s_thr = reinterpret_cast<uint32_t*>(s_glthr + nthr);
   const GroupDesc& GL = P.groups[P.ngroups - 1];
   for (int k = t; k < per_thr; k += nthr)
     s_gchunk[k] = deposit(uint64_t(k) * nthr << M::SH, P.tile);
@@ -425,6 +430,8 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   // (the last group's lanes run over the lowest tile bits, so the direct
   // stores coalesce)
   s_glthr[t] = deposit(deposit(t, GL.thr), P.tile);
+  for (int g = 0; g < P.ngroups && g < kThrCache; ++g)
+    s_thr[g * nthr + t] = uint32_t(deposit(t, P.groups[g].thr));
   __syncthreads();
   const uint64_t gt = deposit(uint64_t(t) << M::SH, P.tile);
   const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(buf[0]));
@@ -452,7 +459,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
       const bool last = g == P.ngroups - 1;
-      const uint32_t thr = uint32_t(deposit(t, G.thr));
+      const uint32_t thr = g < kThrCache ? s_thr[g * nthr + t] : uint32_t(deposit(t, G.thr));
       // per register bit: the offset change of setting that bit (swizzled slot
       // part and in-slot part occupy disjoint bits, so they combine by XOR and
       // so do the bits of an element index)
@@ -559,7 +566,8 @@ int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
   if (g_num_sms == 0) HS_CUDA(cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev));
   const int threads = 1 << (P.m - R);
   const int per_thr = ((1 << P.m) * int(sizeof(V)) / 16) / threads;
-  const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(uint64_t) * (per_thr + R + threads);
+  const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(uint64_t) * (per_thr + R + threads) +
+                      sizeof(uint32_t) * kThrCache * threads;
   if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K1 tile of 2^%d needs %zu B", P.m, smem);
   int per_sm = 0;
   HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, V>, threads, smem));
