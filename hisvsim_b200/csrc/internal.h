@@ -129,8 +129,8 @@ int current_tile_hint();  // hs_set_tile_qubits' value
 // 3 = 8 amplitudes (default), 4 = 16 amplitudes); complex64 programs always
 // use 4
 int k1_reg_bits(int dtype);
-// complex128 tiles stop at 2^11 so that three CTAs (two 32 KiB buffers each,
-// <= 168 registers per thread) share an SM; complex64 tiles go to 2^12
+// complex128 tiles stop at 2^11 (two 32 KiB buffers per CTA); complex64
+// tiles go to 2^12
 inline int max_tile_bits(int dtype) { return dtype == HS_DTYPE_C64 ? 12 : 11; }
 
 // ---- K2 bit-swap program ----------------------------------------------------
