@@ -59,6 +59,21 @@ def test_tile_hint_bounds():
     assert abi.set_k1_reg_bits(prev) == 4
 
 
+def test_fused_knob_bounds():
+    """K4 variant and fused pass shape: defaults (bulk-loaded, one unitary
+    per pass on 2^13 tiles) and the rejected values."""
+    assert abi.lib().hs_set_k4_variant(3) == abi.HS_E_INVALID
+    assert abi.lib().hs_set_k4_variant(-1) == abi.HS_E_INVALID
+    prev = abi.set_k4_variant(1)
+    assert prev == 2
+    assert abi.set_k4_variant(prev) == 1
+    assert abi.lib().hs_set_fused_shape(1, 14) == abi.HS_E_INVALID
+    assert abi.lib().hs_set_fused_shape(2, 13) == abi.HS_E_INVALID
+    prev = abi.set_fused_shape(2, 12)
+    assert prev == 113
+    assert abi.set_fused_shape(prev // 100, prev % 100) == 212
+
+
 def test_pymod_surface():
     from hisvsim_b200 import svsimulator_py_wrapper as sv
 
