@@ -312,9 +312,25 @@ __device__ __forceinline__ void op_inplace(V (&v)[1 << R], const DevOp& op, cons
   case 64 + (P): if constexpr (FULL && (JB) < R) d2c<R, JA, JB, false>(v, c, 0u, true); break;
 #define DR(J) \
   case 88 + (J): if constexpr ((J) < R) d1r<R, J>(v, c); break;
-  switch (op.code) {
-    D1(0) D1(1) D1(2) D1(3)
-    DR(0) DR(1) DR(2) DR(3)
+  // the most frequent ops first (uncontrolled dense one-qubit gates, with a
+  // real top-left coefficient or general), so that their dispatch takes two
+  // short tests instead of a search over every code
+  const int code = op.code;
+  if (code >= 88) {
+    switch (code) {
+      DR(0) DR(1) DR(2) DR(3)
+      default: break;
+    }
+    return;
+  }
+  if (code < 4) {
+    switch (code) {
+      D1(0) D1(1) D1(2) D1(3)
+      default: break;
+    }
+    return;
+  }
+  switch (code) {
     D2(0, 0, 1) D2(1, 0, 2) D2(2, 0, 3) D2(3, 1, 2) D2(4, 1, 3) D2(5, 2, 3)
     C1(0) C1(1) C1(2) C1(3)
     case 16:  // sign flip of every element of the thread (mask outside the registers)
