@@ -27,7 +27,7 @@ int set_error(int code, const char* fmt, ...) {
 static std::atomic<long long> g_gates{0}, g_passes{0}, g_param_bytes{0};
 static std::atomic<int> g_tile_hint{0};
 int current_tile_hint() { return g_tile_hint.load(); }
-static std::atomic<int> g_k1_rbits{3};
+static std::atomic<int> g_k1_rbits{4};
 int k1_reg_bits(int dtype) { return dtype == HS_DTYPE_C128 ? g_k1_rbits.load() : kRegBits; }
 
 // device-time accounting of K1/K2 launches: event pairs resolved when read
@@ -333,8 +333,21 @@ int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets
   for (int p = 0; p < num_parts; ++p)
     HS_TRY(lower_all(st, gates + part_offsets[p], part_offsets[p + 1] - part_offsets[p],
                      &all[p]));
-  for (int p = 0; p < num_parts; ++p)
-    HS_TRY(run_lowered(st, all[p], part_offsets[p + 1] - part_offsets[p], S(stream)));
+  // one pass (or more) per part; the pending diagonal of the factored
+  // rotations is carried from part to part and applied by the last one
+  Frames fr;
+  fr.reset(st->n);
+  std::vector<PartProgram> progs;
+  for (int p = 0; p < num_parts; ++p) {
+    HS_TRY(plan_gates(st->n, st->q2s, all[p], &fr, p == num_parts - 1, g_tile_hint.load(),
+                      st->dtype, &progs));
+    TimedRegion tr(S(stream));
+    for (const auto& pr : progs) {
+      HS_TRY(launch_part(st->amp, st->dtype, pr, S(stream)));
+      count_pass(pr.nops);
+      g_param_bytes += (long long)sizeof(PartProgram);
+    }
+  }
   return HS_OK;
 }
 
@@ -349,10 +362,13 @@ int hs_parts_run_timed(hs_state* st, const hs_gate* gates, const int32_t* part_o
   // plan every part before the first launch, so that the device never waits
   // for the host between two parts and each event pair brackets one part only
   std::vector<std::vector<PartProgram>> progs(num_parts);
+  Frames fr;
+  fr.reset(st->n);
   for (int p = 0; p < num_parts; ++p) {
     std::vector<LoweredGate> lg;
     HS_TRY(lower_all(st, gates + part_offsets[p], part_offsets[p + 1] - part_offsets[p], &lg));
-    HS_TRY(plan_part(st->n, st->q2s, lg, g_tile_hint.load(), st->dtype, &progs[p]));
+    HS_TRY(plan_gates(st->n, st->q2s, lg, &fr, p == num_parts - 1, g_tile_hint.load(),
+                      st->dtype, &progs[p]));
   }
   std::vector<cudaEvent_t> ev(num_parts + 1, nullptr);
   int rc = HS_OK;
@@ -396,7 +412,8 @@ int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates
     m = std::max(m, int(p.m));
     for (int i = 0; i < p.nops; ++i) {
       diag += p.ops[i].kind >= OPD_PHASE;
-      dense += p.ops[i].kind == OP1_DENSE || p.ops[i].kind == OP2_DENSE;
+      dense += p.ops[i].kind == OP1_ROT || p.ops[i].kind == OP1_DENSE ||
+               p.ops[i].kind == OP2_DENSE;
     }
   }
   stats[0] = int32_t(progs.size());

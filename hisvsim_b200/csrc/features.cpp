@@ -98,7 +98,8 @@ int features_of(int n, int dtype, const Lowered& L, const int32_t* idx, int len,
       m = std::max(m, int(p.m));
       for (int i = 0; i < p.nops; ++i) {
         diag += p.ops[i].kind >= OPD_PHASE;
-        dense += p.ops[i].kind == OP1_DENSE || p.ops[i].kind == OP2_DENSE;
+        dense += p.ops[i].kind == OP1_ROT || p.ops[i].kind == OP1_DENSE ||
+                 p.ops[i].kind == OP2_DENSE;
       }
     }
     f[9] = float(progs.size()) / 4.f;

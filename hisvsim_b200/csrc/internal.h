@@ -50,42 +50,60 @@ constexpr int kMaxOps = 128;
 constexpr int kMaxCoef = 640;      // complex coefficients (double2)
 constexpr int kMaxGroups = 48;
 constexpr int kMaxRuns = 16;
+constexpr int kMaxFlush = 64;      // thread / outer entries of the frame flushes of a program
+constexpr int kMaxRounds = 128;
 
+// What an op does (planner statistics and the features of the learned form).
 enum OpKind : uint8_t {
-  // gates whose targets must be register bits
-  OP1_DENSE = 0,  // 2x2
-  OP1_X = 1,      // [[0,1],[1,0]]
-  OP1_H = 2,      // s*[[1,1],[1,-1]], s = 1/sqrt(2)
-  OP1_Y = 3,      // [[0,-i],[i,0]]
+  OP1_ROT = 0,    // uncontrolled one-qubit rotation RY RZ as shears (K1 codes zy / y)
+  OP1_DENSE = 1,  // general 2x2, uncontrolled or controlled
   OP2_DENSE = 4,  // 4x4
   OP2_SWAP = 5,   // swap |01>,|10>
-  // diagonal gates: targets anywhere (register, thread or outer bits)
+  // diagonal ops: targets anywhere (register, thread or outer bits)
   OPD_PHASE = 8,  // multiply by c0 where every bit of the mask is 1
   OPD_NEG = 9,    // negate where every bit of the mask is 1
   OPD_DIAG = 10,  // multiply by c[b0 | b1 << 1] where the control mask holds
+  OPD_FLUSH = 11, // multiply by G * prod over listed thread/outer bits b set of r_b
 };
-// dispatch codes (kernel switch):
-//   1q dense, uncontrolled (v -> other array):      0 + ja           (0..3)
-//   1q dense, controlled (in place):                 4 + ja           (4..7)
-//   diagonal sign flip, register mask p (in place): 16 + p           (16..31)
-//   diagonal phase, register mask p (in place):     32 + p           (32..47)
-//   general diagonal (in place):                    48
-//   2q dense, uncontrolled (v -> other array):      64 + pair        (64..69)
-//   2q dense, controlled (in place):                72 + pair        (72..77)
-//   2q swap (in place):                             80 + pair        (80..85)
-//   1q dense, uncontrolled, real top-left (in place): 88 + ja        (88..91)
+
+// K1 dispatch codes (one dense range).  j = register position of the
+// target, M = register mask.
+//   rotation RY(theta) RZ(beta) on register bit j:   kc_zy + j
+//   rotation RY(theta) alone:                        kc_y + j
+//   general 2x2, uncontrolled:                       kc_d1 + j
+//   general 2x2, controlled:                         kc_c1 + j
+//   sign flip, register mask M:                      kc_neg + M   (M = 0: whole thread, deferred)
+//   phase c0, register mask M:                       kc_ph + M
+//   general diagonal:                                kc_diag
+//   4x4 uncontrolled / controlled / swap, register pair p: kc_d2 / kc_c2 / kc_sw + p
+//   frame flush:                                     kc_flush
+enum K1Code : uint8_t {
+  kc_zy = 0,
+  kc_y = 4,
+  kc_d1 = 8,
+  kc_c1 = 12,
+  kc_neg = 16,
+  kc_ph = 32,
+  kc_diag = 48,
+  kc_d2 = 49,
+  kc_c2 = 55,
+  kc_sw = 61,
+  kc_flush = 67,
+  kc_count = 68,
+};
 enum TargetWhere : uint8_t { TW_NONE = 0, TW_REG = 1, TW_THR = 2, TW_OUT = 3 };
 
 struct DevOp {
-  uint8_t kind;
-  uint8_t code;
+  uint8_t kind;               // OpKind
+  uint8_t code;               // K1Code
   uint8_t ja, jb;             // register positions of non-diagonal targets (ja < jb)
   uint8_t t0w, t0p, t1w, t1p;  // diagonal targets: where (TargetWhere) and position
   uint16_t coef;              // first coefficient (index into PartProgram::coef)
   uint16_t creg;              // control/mask bits that are register bits (element space)
   uint32_t cthr;              // control/mask bits that are thread bits (tile-index space)
   uint64_t couter;            // control/mask bits outside the tile (global index space)
-  uint64_t pad;
+  uint16_t fl_first, fl_n;    // flush: entries [fl_first, fl_first + fl_n) of flw/flp
+  uint32_t pad;
 };
 static_assert(sizeof(DevOp) == 32, "DevOp layout");
 
@@ -96,9 +114,24 @@ struct Runs {  // bit-run deposit: out |= ((x >> src) & (2^len - 1)) << dst
   uint8_t dst[kMaxRuns];
 };
 
+// A round of a register group: at most one rotation per register bit j (bit
+// j of `mask`; with an RZ part when bit j of `zmask` is set; coefficients at
+// coef[cidx[j]]), applied in the order j = 0, 1, ..., then the ops
+// ops[first_other, first_other + num_other).  The planner packs a group's ops
+// into rounds without changing their order where they do not commute.
+struct RoundDesc {
+  uint8_t mask, zmask;
+  uint16_t first_other, num_other;
+  uint16_t cidx[kRegBits];
+  uint16_t pad;
+};
+static_assert(sizeof(RoundDesc) == 16, "RoundDesc layout");
+
 struct GroupDesc {
   uint8_t reg_tbit[kRegBits];  // tile bit held by register bit j
-  uint16_t first_op, num_ops;
+  uint32_t dx[kRegBits];       // shared-memory byte-offset change of setting register bit j
+  uint16_t first_op, num_ops;  // every op of the group (rotations included), in order
+  uint16_t first_round, num_rounds;
   Runs thr;                    // thread index -> tile index
 };
 
@@ -113,21 +146,47 @@ struct PartProgram {
   Runs tile;           // tile index -> global index
   Runs outer;          // tile number -> global index
   uint8_t tile_slot[16];  // global slot of tile bit b
+  int32_t nfl;         // used entries of flw / flp
+  uint8_t flw[kMaxFlush], flp[kMaxFlush];  // flush entries: where (TW_THR / TW_OUT), position
+  int32_t nrounds, nothers;
   GroupDesc groups[kMaxGroups];
-  DevOp ops[kMaxOps];
+  DevOp ops[kMaxOps];            // per group: rotations and others in program order
+  uint16_t others[kMaxOps];      // per round: indices into ops of its non-rotation ops
+  RoundDesc rounds[kMaxRounds];
   double2 coef[kMaxCoef];
 };
 static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
 
+// Pending diagonal of a state under planning: the true state is
+// G * (prod_q diag(1, r[q]) on qubit q) * (the stored amplitudes).  Uncontrolled
+// one-qubit gates are applied as rotations in factored form, and the phases
+// and scale factors they leave are carried here instead of being applied
+// (they commute with every diagonal gate and are absorbed by the next
+// one-qubit gate on the same qubit); a flush applies them.
+struct Frames {
+  std::vector<cplx> r;   // per qubit
+  cplx G{1.0, 0.0};
+  void reset(int n) {
+    r.assign(n, cplx(1.0, 0.0));
+    G = cplx(1.0, 0.0);
+  }
+  bool identity() const;
+};
+
 // Build the K1 programs for a sequence of lowered gates on a state whose
-// qubit q sits in slot q2s[q].  Long parts produce several programs (each one
-// state pass).  Returns HS_OK or an error.
+// qubit q sits in slot q2s[q].  `fr` carries the pending diagonal in and out;
+// with `flush` the last program applies it (fr becomes the identity).  Long
+// parts produce several programs (each one state pass).  Returns HS_OK or an
+// error.
+int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
+               Frames* fr, bool flush, int tile_bits_hint, int dtype,
+               std::vector<PartProgram>* programs);
+// one self-contained part: fresh frames, flushed at the end
 int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
               int tile_bits_hint, int dtype, std::vector<PartProgram>* programs);
 int current_tile_hint();  // hs_set_tile_qubits' value
-// register bits per thread of K1's complex128 programs (hs_set_k1_reg_bits:
-// 3 = 8 amplitudes (default), 4 = 16 amplitudes); complex64 programs always
-// use 4
+// register bits per thread of K1 programs (hs_set_k1_reg_bits: 4 = 16
+// amplitudes (default), 3 = 8 amplitudes)
 int k1_reg_bits(int dtype);
 // complex128 tiles stop at 2^11 (two 32 KiB buffers per CTA); complex64
 // tiles go to 2^12

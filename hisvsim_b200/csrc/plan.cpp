@@ -1,4 +1,5 @@
-// Host planner for K1: turns one part (a gate sequence) into tile programs.
+// Host planner for K1: turns a gate sequence (one part, or the parts of one
+// call) into tile programs.
 //
 // The reference runs a part by gathering, for each assignment of the outer
 // qubits, the 2^k amplitudes of the part's qubits into an inner state vector,
@@ -15,6 +16,24 @@
 // index bits, so they run in any layout and their qubits need not be in the
 // tile at all.  Controls are index predicates wherever their bits are, as
 // control_offset is in StateVector::apply (state_vector.hpp:410-417).
+//
+// Before that, the gate sequence is rewritten (Frames, internal.h): an
+// uncontrolled one-qubit gate U on qubit q, preceded by the pending diagonal
+// diag(1, r_q), is factored (Z-Y-Z Euler form) as
+//     U diag(1, r_q) = diag(a0, a1) * RY(theta) * diag(1, e^{i beta}),
+// with |beta| <= pi/2 (otherwise Z = diag(1, -1) moves to the left factor:
+// RY(theta) Z = Z RY(-theta)).  RY(theta) diag(1, e^{i beta}) is applied as
+// exact plane rotations, each written as three in-place shears (x -= t y;
+// y += s x; x -= t y, with t = tan(angle/2), s = sin(angle)): the phase turns
+// the (re, im) plane of the pair's second amplitude by beta, RY the (first,
+// second) plane of the pair's real and of its imaginary parts by theta/2.
+// 9 FP64 FMA per amplitude pair (6 without the phase), every one updating a
+// register in place, so the kernel's op dispatch needs no register moves.
+// diag(a0, a1) joins the pending diagonal, which commutes with every diagonal
+// gate (CZ, phases) and is absorbed by the next one-qubit gate on q.
+// Diagonal one-qubit gates (S, T, RZ, ...) only update the pending diagonal.
+// Whatever is pending at the end of a call is applied by one flush op.  The
+// result is the reference's state up to rounding.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -23,6 +42,14 @@
 #include "internal.h"
 
 namespace hisv {
+
+bool Frames::identity() const {
+  if (G != cplx(1.0, 0.0)) return false;
+  for (const auto& x : r)
+    if (x != cplx(1.0, 0.0)) return false;
+  return true;
+}
+
 namespace {
 
 void build_runs(const std::vector<int>& dst_of_src, Runs* r) {
@@ -51,17 +78,203 @@ bool is_diagonal(const LoweredGate& g) {
   return true;
 }
 
+// ---- the factored rotation ---------------------------------------------------
+struct Rot {
+  bool has_z;        // phase part present (beta != 0)
+  double tz, sz;     // shears of the phase: tan(beta/2), sin(beta)
+  double ty, sy;     // shears of RY: tan(theta/4), sin(theta/2)
+  cplx a0, a1;       // left diagonal (the new pending diagonal of the qubit)
+};
+
+// W = diag(a0, a1) * [[c, -s], [s, c]] * diag(1, b1), c = |W00|, s = |W10|
+// (c = cos(theta/2), s = sin(theta/2), theta in [0, pi]; b1 = e^{i beta}).
+// False when W is not unitary to 1e-12 (custom C1 matrices need not be).
+bool factor_rotation(const cplx* W, Rot* R) {
+  const double c = std::abs(W[0]), s = std::abs(W[2]);
+  const double c1 = std::abs(W[3]), s1 = std::abs(W[1]);
+  const double tol = 1e-12;
+  if (std::fabs(c * c + s * s - 1.0) > tol || std::fabs(c1 * c1 + s1 * s1 - 1.0) > tol ||
+      std::abs(std::conj(W[0]) * W[1] + std::conj(W[2]) * W[3]) > tol)
+    return false;
+  cplx a0, a1, b1;
+  double cc = c, ss = s;
+  if (c > 0.0 && s > 0.0) {
+    a0 = W[0] / c;
+    a1 = W[2] / s;
+    b1 = c >= s ? W[3] / (a1 * c) : -W[1] / (a0 * s);
+    b1 /= std::abs(b1);
+  } else if (c == 0.0) {  // anti-diagonal
+    a0 = -W[1];
+    a1 = W[2];
+    b1 = 1.0;
+    cc = 0.0;
+    ss = 1.0;
+  } else {
+    return false;  // diagonal: handled by the caller
+  }
+  // the norms of the rows are 1 to 1e-12; keep the left diagonal unit-modulus
+  a0 /= std::abs(a0);
+  a1 /= std::abs(a1);
+  const double nrm = std::hypot(cc, ss);
+  cc /= nrm;
+  ss /= nrm;
+  double sign = 1.0;
+  if (b1.real() < 0.0) {
+    // RY(theta) diag(1, b1) = Z RY(-theta) diag(1, -b1): |arg(-b1)| <= pi/2
+    b1 = -b1;
+    a1 = -a1;
+    sign = -1.0;
+  }
+  R->a0 = a0;
+  R->a1 = a1;
+  // tan(theta/4) = s / (1 + c) (half-angle formula for theta/2, c >= 0)
+  R->ty = sign * ss / (1.0 + cc);
+  R->sy = sign * ss;
+  R->has_z = !(b1.real() == 1.0 && b1.imag() == 0.0);
+  // tan(beta/2) = sin(beta) / (1 + cos(beta)), cos(beta) >= 0
+  R->tz = R->has_z ? b1.imag() / (1.0 + b1.real()) : 0.0;
+  R->sz = R->has_z ? b1.imag() : 0.0;
+  return true;
+}
+
+// ---- rewritten gates -----------------------------------------------------------
+enum RKind { RK_MATRIX = 0, RK_ROT = 1, RK_FLUSH = 2 };
+
+struct RGate {
+  RKind kind = RK_MATRIX;
+  LoweredGate g;              // targets / controls (and the matrix for RK_MATRIX)
+  Rot rot;                    // RK_ROT
+  std::vector<int> flq;       // RK_FLUSH: qubits
+  std::vector<cplx> flr;      //           their factors r_q (applied where the bit is 1)
+  cplx flG{1.0, 0.0};         //           global factor
+};
+
+bool is_swap4(const cplx* m) {
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c) {
+      const bool one = (r == 0 && c == 0) || (r == 3 && c == 3) || (r == 1 && c == 2) ||
+                       (r == 2 && c == 1);
+      if (!exact(m[4 * r + c], one ? 1.0 : 0.0)) return false;
+    }
+  return true;
+}
+
+// phase r on the |1> of qubit q, as a diagonal one-qubit gate
+RGate phase_gate(int q, cplx r) {
+  RGate x;
+  x.g.nt = 1;
+  x.g.targets[0] = q;
+  x.g.nc = 0;
+  x.g.m[0] = 1.0;
+  x.g.m[1] = x.g.m[2] = 0.0;
+  x.g.m[3] = r;
+  return x;
+}
+
+RGate flush_gate(Frames* F) {
+  RGate x;
+  x.kind = RK_FLUSH;
+  x.g.nt = 0;
+  x.g.nc = 0;
+  for (int q = 0; q < int(F->r.size()); ++q)
+    if (F->r[q] != cplx(1.0, 0.0)) {
+      x.flq.push_back(q);
+      x.flr.push_back(F->r[q]);
+      F->r[q] = 1.0;
+    }
+  x.flG = F->G;
+  F->G = 1.0;
+  return x;
+}
+
+void rewrite(const std::vector<LoweredGate>& in, Frames* F, std::vector<RGate>* out) {
+  for (const auto& g : in) {
+    if (g.nt == 0) continue;
+    const bool diag = is_diagonal(g);
+    if (g.nt == 1 && g.nc == 0) {
+      const int q = g.targets[0];
+      const cplx rq = F->r[q];
+      if (diag) {
+        if (g.m[0] != cplx(0.0, 0.0)) {  // joins the pending diagonal
+          F->G *= g.m[0];
+          F->r[q] = g.m[3] * rq / g.m[0];
+        } else {  // degenerate (custom C1): applied with the pending factor
+          RGate x;
+          x.g = g;
+          x.g.m[3] *= rq;
+          F->r[q] = 1.0;
+          out->push_back(x);
+        }
+        continue;
+      }
+      cplx W[4] = {g.m[0], g.m[1] * rq, g.m[2], g.m[3] * rq};
+      RGate x;
+      x.g = g;
+      if (factor_rotation(W, &x.rot)) {
+        x.kind = RK_ROT;
+        F->G *= x.rot.a0;
+        F->r[q] = x.rot.a1 / x.rot.a0;
+      } else {
+        for (int k = 0; k < 4; ++k) x.g.m[k] = W[k];
+        F->r[q] = 1.0;
+      }
+      out->push_back(x);
+      continue;
+    }
+    if (diag) {  // controlled or two-qubit diagonal: commutes with the pending diagonal
+      RGate x;
+      x.g = g;
+      out->push_back(x);
+      continue;
+    }
+    if (g.nt == 2 && g.nc == 0) {
+      const int t0 = g.targets[0], t1 = g.targets[1];
+      RGate x;
+      x.g = g;
+      if (is_swap4(g.m)) {
+        std::swap(F->r[t0], F->r[t1]);
+      } else {
+        // absorb diag(1, r_t0) (x) diag(1, r_t1); reference index i = 2*b(t0) + b(t1)
+        for (int c = 0; c < 4; ++c) {
+          cplx d = 1.0;
+          if (c & 2) d *= F->r[t0];
+          if (c & 1) d *= F->r[t1];
+          for (int r = 0; r < 4; ++r) x.g.m[4 * r + c] *= d;
+        }
+        F->r[t0] = F->r[t1] = 1.0;
+      }
+      out->push_back(x);
+      continue;
+    }
+    // controlled non-diagonal gate: apply the pending factors of its targets first
+    for (int i = 0; i < g.nt; ++i) {
+      const int t = g.targets[i];
+      if (F->r[t] != cplx(1.0, 0.0)) {
+        out->push_back(phase_gate(t, F->r[t]));
+        F->r[t] = 1.0;
+      }
+    }
+    RGate x;
+    x.g = g;
+    out->push_back(x);
+  }
+}
+
+// ---- slot view -------------------------------------------------------------------
 struct SlotGate {
-  const LoweredGate* g;
+  const RGate* rg;
   bool diag;
-  int ts[2];  // target slots
-  int nc;
-  int cs[HS_MAX_CONTROLS];
+  int nt;
+  int ts[2];                 // non-diagonal target slots
+  std::vector<int> slots;    // every slot the gate touches (dependencies)
 };
 
 int coef_count(const SlotGate& sg) {
+  const RGate& r = *sg.rg;
+  if (r.kind == RK_ROT) return 2;
+  if (r.kind == RK_FLUSH) return 1 + int(r.flq.size());
   if (sg.diag) return 4;
-  return sg.g->nt == 1 ? 4 : 16;
+  return r.g.nt == 1 ? 4 : 16;
 }
 
 struct Layout {
@@ -95,62 +308,66 @@ void add_mask_bit(const Layout& L, int slot, DevOp* op) {
     op->cthr |= 1u << p;
 }
 
-void emit_op(const SlotGate& sg, const Layout& L, PartProgram* P) {
-  DevOp op;
-  std::memset(&op, 0, sizeof(op));
-  for (int i = 0; i < sg.nc; ++i) add_mask_bit(L, sg.cs[i], &op);
-  const cplx* m = sg.g->m;
-  int base = P->ncoef;  // coefficients are appended in op order
-  auto push = [&](cplx c) {
-    P->coef[base].x = c.real();
-    P->coef[base].y = c.imag();
-    ++base;
-  };
-  op.coef = uint16_t(base);
+struct Emitter {
+  PartProgram* P;
+  const std::vector<int>* q2s;
+  void push(cplx c) {
+    P->coef[P->ncoef].x = c.real();
+    P->coef[P->ncoef].y = c.imag();
+    ++P->ncoef;
+  }
+  void add(const DevOp& op) { P->ops[P->nops++] = op; }
+  DevOp blank() {
+    DevOp op;
+    std::memset(&op, 0, sizeof(op));
+    op.coef = uint16_t(P->ncoef);
+    return op;
+  }
+};
+
+void emit_matrix(const SlotGate& sg, const Layout& L, Emitter& E) {
+  const LoweredGate& g = sg.rg->g;
+  DevOp op = E.blank();
+  for (int i = 0; i < g.nc; ++i) add_mask_bit(L, (*E.q2s)[g.controls[i]], &op);
+  const cplx* m = g.m;
   const bool ctrl = op.creg != 0 || op.cthr != 0 || op.couter != 0;
   if (sg.diag) {
-    if (sg.g->nt == 1 && exact(m[0], 1)) {
+    const int s0 = (*E.q2s)[g.targets[0]];
+    if (g.nt == 1 && exact(m[0], 1)) {
       // phase on the |1> of the target: a mask over controls + target
-      add_mask_bit(L, sg.ts[0], &op);
+      add_mask_bit(L, s0, &op);
       if (exact(m[3], -1)) {
         op.kind = OPD_NEG;
+        op.code = uint8_t(kc_neg + op.creg);
       } else {
         op.kind = OPD_PHASE;
-        push(m[3]);
+        op.code = uint8_t(kc_ph + op.creg);
+        E.push(m[3]);
       }
     } else {
       op.kind = OPD_DIAG;
-      locate(L, sg.ts[0], &op.t0w, &op.t0p);
-      if (sg.g->nt == 1) {
-        push(m[0]);
-        push(m[3]);
+      op.code = kc_diag;
+      locate(L, s0, &op.t0w, &op.t0p);
+      if (g.nt == 1) {
+        E.push(m[0]);
+        E.push(m[3]);
       } else {
         // device index q = b(t0) | b(t1) << 1; reference index i = 2*b(t0) + b(t1)
-        locate(L, sg.ts[1], &op.t1w, &op.t1p);
-        push(m[0]);   // q=0: i=0
-        push(m[10]);  // q=1: b0=1,b1=0 -> i=2
-        push(m[5]);   // q=2: b0=0,b1=1 -> i=1
-        push(m[15]);  // q=3: i=3
+        locate(L, (*E.q2s)[g.targets[1]], &op.t1w, &op.t1p);
+        E.push(m[0]);   // q=0: i=0
+        E.push(m[10]);  // q=1: b0=1,b1=0 -> i=2
+        E.push(m[5]);   // q=2: b0=0,b1=1 -> i=1
+        E.push(m[15]);  // q=3: i=3
       }
     }
-    if (op.kind == OPD_NEG)
-      op.code = uint8_t(16 + op.creg);
-    else if (op.kind == OPD_PHASE)
-      op.code = uint8_t(32 + op.creg);
-    else
-      op.code = 48;
-  } else if (sg.g->nt == 1) {
+  } else if (g.nt == 1) {
     uint8_t w;
     locate(L, sg.ts[0], &w, &op.ja);
-    // every non-diagonal one-target gate runs as a dense 2x2 (X, Y and H
-    // included: multiplying by 0 and +-1 is exact, H differs from
-    // s*(a+b) by at most one rounding)
     op.kind = OP1_DENSE;
-    for (int k = 0; k < 4; ++k) push(m[k]);
-    op.code = uint8_t((ctrl ? 4 : 0) + op.ja);
+    for (int k = 0; k < 4; ++k) E.push(m[k]);
+    op.code = uint8_t((ctrl ? kc_c1 : kc_d1) + op.ja);
   } else {
-    uint8_t w;
-    uint8_t p0, p1;
+    uint8_t w, p0, p1;
     locate(L, sg.ts[0], &w, &p0);
     locate(L, sg.ts[1], &w, &p1);
     op.ja = std::min(p0, p1);
@@ -160,91 +377,210 @@ void emit_op(const SlotGate& sg, const Layout& L, PartProgram* P) {
     cplx md[16];
     for (int qo = 0; qo < 4; ++qo)
       for (int qi = 0; qi < 4; ++qi) md[4 * qo + qi] = m[4 * ref_index(qo) + ref_index(qi)];
-    bool swap = true;
-    for (int r = 0; r < 4; ++r)
-      for (int c = 0; c < 4; ++c) {
-        const bool one = (r == 0 && c == 0) || (r == 3 && c == 3) || (r == 1 && c == 2) ||
-                         (r == 2 && c == 1);
-        if (!exact(md[4 * r + c], one ? 1.0 : 0.0)) swap = false;
-      }
-    if (swap) {
-      op.kind = OP2_SWAP;
-    } else {
-      op.kind = OP2_DENSE;
-      for (int k = 0; k < 16; ++k) push(md[k]);
-    }
     static const int pair_index[4][4] = {{-1, 0, 1, 2}, {-1, -1, 3, 4}, {-1, -1, -1, 5},
                                          {-1, -1, -1, -1}};
-    op.code = uint8_t((op.kind == OP2_SWAP ? 80 : (ctrl ? 72 : 64)) + pair_index[op.ja][op.jb]);
+    const int pi = pair_index[op.ja][op.jb];
+    if (is_swap4(md)) {
+      op.kind = OP2_SWAP;
+      op.code = uint8_t(kc_sw + pi);
+    } else {
+      op.kind = OP2_DENSE;
+      for (int k = 0; k < 16; ++k) E.push(md[k]);
+      op.code = uint8_t((ctrl ? kc_c2 : kc_d2) + pi);
+    }
   }
-  P->ncoef = base;
-  P->ops[P->nops++] = op;
+  E.add(op);
+}
+
+void emit_rot(const SlotGate& sg, const Layout& L, Emitter& E) {
+  DevOp op = E.blank();
+  uint8_t w;
+  locate(L, sg.ts[0], &w, &op.ja);
+  const Rot& r = sg.rg->rot;
+  op.kind = OP1_ROT;
+  op.code = uint8_t((r.has_z ? kc_zy : kc_y) + op.ja);
+  E.push(cplx(r.ty, r.sy));
+  if (r.has_z) E.push(cplx(r.tz, r.sz));
+  E.add(op);
+}
+
+// register-bit factors become phase ops; thread / outer ones and G one flush op
+int emit_flush(const SlotGate& sg, const Layout& L, Emitter& E) {
+  const RGate& r = *sg.rg;
+  std::vector<int> rest;
+  for (size_t i = 0; i < r.flq.size(); ++i) {
+    uint8_t w, p;
+    locate(L, (*E.q2s)[r.flq[i]], &w, &p);
+    if (w == TW_REG) {
+      DevOp op = E.blank();
+      op.kind = OPD_PHASE;
+      op.creg = uint16_t(1u << p);
+      op.code = uint8_t(kc_ph + op.creg);
+      E.push(r.flr[i]);
+      E.add(op);
+    } else {
+      rest.push_back(int(i));
+    }
+  }
+  if (rest.empty() && r.flG == cplx(1.0, 0.0)) return HS_OK;
+  PartProgram* P = E.P;
+  if (P->nfl + int(rest.size()) > kMaxFlush)
+    return set_error(HS_E_UNSUPPORTED, "frame flush of %d entries exceeds %d", int(rest.size()),
+                     kMaxFlush);
+  DevOp op = E.blank();
+  op.kind = OPD_FLUSH;
+  op.code = kc_flush;
+  op.fl_first = uint16_t(P->nfl);
+  op.fl_n = uint16_t(rest.size());
+  E.push(r.flG);
+  for (int i : rest) {
+    uint8_t w, p;
+    locate(L, (*E.q2s)[r.flq[i]], &w, &p);
+    P->flw[P->nfl] = w;
+    P->flp[P->nfl] = p;
+    ++P->nfl;
+    E.push(r.flr[i]);
+  }
+  E.add(op);
+  return HS_OK;
+}
+
+// does op x act on register bit j (target, control or mask)?
+bool touches_reg(const DevOp& x, int j) {
+  if (x.kind == OP1_ROT || x.kind == OP1_DENSE) {
+    if (x.ja == j) return true;
+  } else if (x.kind == OP2_DENSE || x.kind == OP2_SWAP) {
+    if (x.ja == j || x.jb == j) return true;
+  } else if (x.kind == OPD_DIAG) {
+    if ((x.t0w == TW_REG && x.t0p == j) || (x.t1w == TW_REG && x.t1p == j)) return true;
+  }
+  return ((x.creg >> j) & 1) != 0;
+}
+
+bool diagonal_op(const DevOp& x) { return x.kind >= OPD_PHASE; }
+
+// Pack the group's ops into rounds (RoundDesc) by list scheduling: op b must
+// follow an earlier op a only when both act on a common register bit and not
+// both are diagonal (ops act non-diagonally on register bits alone, so
+// anything else commutes).  Each round takes, per register bit, the first
+// rotation whose predecessors are all in earlier rounds, then every other op
+// whose predecessors are scheduled (this round's rotations included), in
+// program order.
+void build_rounds(PartProgram* P, GroupDesc* gd) {
+  gd->first_round = uint16_t(P->nrounds);
+  const int o0 = gd->first_op, n = gd->num_ops;
+  std::vector<uint16_t> regs(n, 0);  // register bits each op acts on
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < kRegBits; ++j)
+      if (touches_reg(P->ops[o0 + i], j)) regs[i] |= uint16_t(1u << j);
+  std::vector<std::vector<int>> preds(n);
+  for (int b = 0; b < n; ++b)
+    for (int a = 0; a < b; ++a)
+      if ((regs[a] & regs[b]) && !(diagonal_op(P->ops[o0 + a]) && diagonal_op(P->ops[o0 + b])))
+        preds[b].push_back(a);
+  // 0: unscheduled, 1: in an earlier round, 2: in this round
+  std::vector<int> state(n, 0);
+  int left = n;
+  auto ready = [&](int b, int need) {
+    for (int a : preds[b])
+      if (state[a] == 0 || state[a] > need) return false;
+    return true;
+  };
+  while (left > 0) {
+    RoundDesc* rd = &P->rounds[P->nrounds++];
+    std::memset(rd, 0, sizeof(*rd));
+    rd->first_other = uint16_t(P->nothers);
+    for (int b = 0; b < n; ++b) {
+      const DevOp& x = P->ops[o0 + b];
+      if (state[b] || x.kind != OP1_ROT || ((rd->mask >> x.ja) & 1) || !ready(b, 1)) continue;
+      // an earlier unscheduled rotation on the same bit goes first
+      bool first = true;
+      for (int a = 0; a < b; ++a)
+        if (!state[a] && P->ops[o0 + a].kind == OP1_ROT && P->ops[o0 + a].ja == x.ja) first = false;
+      if (!first) continue;
+      rd->mask |= uint8_t(1u << x.ja);
+      if (x.code < kc_y) rd->zmask |= uint8_t(1u << x.ja);
+      rd->cidx[x.ja] = x.coef;
+      state[b] = 2;
+      --left;
+    }
+    for (bool grew = true; grew;) {
+      grew = false;
+      for (int b = 0; b < n; ++b) {
+        if (state[b] || P->ops[o0 + b].kind == OP1_ROT || !ready(b, 2)) continue;
+        P->others[P->nothers++] = uint16_t(o0 + b);
+        ++rd->num_other;
+        state[b] = 2;
+        --left;
+        grew = true;
+      }
+    }
+    for (int b = 0; b < n; ++b)
+      if (state[b] == 2) state[b] = 1;
+  }
+  gd->num_rounds = uint16_t(P->nrounds - gd->first_round);
+}
+
+// XOR-swizzled shared-memory slot (the same function as the kernel's)
+uint32_t swz(uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9) ^ (i >> 12)) & 7u); }
+
+uint32_t smem_dx(int tbit, int dtype) {
+  const int sh = dtype == HS_DTYPE_C64 ? 1 : 0;
+  const uint32_t b = 1u << tbit;
+  return (swz(b >> sh) << 4) ^ ((b & ((1u << sh) - 1u)) * uint32_t(amp_bytes(dtype)));
 }
 
 }  // namespace
 
-// Uncontrolled dense one-qubit ops run with a real top-left coefficient
-// (code 88 + j: two FP64 instructions fewer per amplitude pair): op U becomes
-// e^{-ia} U with a = arg U00, and the program's last uncontrolled dense op,
-// which keeps the general form, absorbs the product of the removed phases (a
-// global phase commutes with every op).  Ops with U00 = 0 keep the general
-// form.
-void factor_phases(PartProgram* P) {
-  int last = -1;
-  for (int i = 0; i < P->nops; ++i)
-    if (P->ops[i].kind == OP1_DENSE && P->ops[i].code < 4) last = i;
-  if (last < 0) return;
-  std::complex<double> g(1.0, 0.0);
-  for (int i = 0; i < last; ++i) {
-    DevOp& op = P->ops[i];
-    if (op.kind != OP1_DENSE || op.code >= 4) continue;
-    double2* c = P->coef + op.coef;
-    const double r = std::hypot(c[0].x, c[0].y);
-    if (!(r > 0.0)) continue;
-    const std::complex<double> f(c[0].x / r, -c[0].y / r);  // e^{-ia}
-    for (int k = 1; k < 4; ++k) {
-      const std::complex<double> v = std::complex<double>(c[k].x, c[k].y) * f;
-      c[k].x = v.real();
-      c[k].y = v.imag();
-    }
-    c[0].x = r;
-    c[0].y = 0.0;
-    g *= std::conj(f);
-    op.code = uint8_t(88 + op.ja);
-  }
-  double2* c = P->coef + P->ops[last].coef;
-  for (int k = 0; k < 4; ++k) {
-    const std::complex<double> v = std::complex<double>(c[k].x, c[k].y) * g;
-    c[k].x = v.real();
-    c[k].y = v.imag();
-  }
-}
-
-int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
-              int tile_bits_hint, int dtype, std::vector<PartProgram>* programs) {
+int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
+               Frames* fr, bool flush, int tile_bits_hint, int dtype,
+               std::vector<PartProgram>* programs) {
   programs->clear();
   if (n < 1 || n > 63) return set_error(HS_E_INVALID, "bad qubit count %d", n);
-  // two tile buffers must fit in shared memory: 2^12 complex128 / 2^13 complex64
+  if (int(fr->r.size()) != n) fr->reset(n);
+  std::vector<RGate> rg;
+  rg.reserve(gates.size() + 2);
+  rewrite(gates, fr, &rg);
+  // keep the carried scale within a few dozen binary orders (it moves only
+  // when non-unitary diagonal gates are absorbed)
+  const double lim = dtype == HS_DTYPE_C64 ? 24.0 : 48.0;
+  if (flush) {
+    if (!fr->identity()) rg.push_back(flush_gate(fr));
+  } else if (std::fabs(std::log2(std::abs(fr->G))) > lim) {
+    Frames scale;
+    scale.G = std::abs(fr->G);
+    rg.push_back(flush_gate(&scale));
+    fr->G /= std::abs(fr->G);
+  }
+  // two tile buffers must fit in shared memory: 2^11 complex128 / 2^12 complex64
   const int max_tile = std::min(n, max_tile_bits(dtype));
-  // automatic size: the largest tile, except complex128 with 8 amplitudes per
-  // thread, whose 2^10 tiles (CTAs of 128 threads, six per SM) hide FP64
-  // latency better than 2^11 (measured)
-  const int auto_m = (dtype == HS_DTYPE_C128 && k1_reg_bits(dtype) == 3) ? 10 : max_tile;
+  const int rbits = k1_reg_bits(dtype);
+  // automatic size: complex128 tiles of 2^10 (CTAs of 64 threads x 16
+  // amplitudes, six per SM), complex64 tiles of 2^12
+  const int auto_m = dtype == HS_DTYPE_C128 ? 10 : max_tile;
   const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : auto_m);
   // keep the lowest slots in the tile so that global accesses come in
   // contiguous runs of at least 64 bytes (complex64 tiles also need slot 0 for
   // their 16-byte chunks)
   const int low_min = std::min(n, dtype == HS_DTYPE_C64 ? 3 : 2);
   std::vector<SlotGate> sgs;
-  for (const auto& g : gates) {
-    if (g.nt == 0) continue;
+  sgs.reserve(rg.size());
+  for (const auto& r : rg) {
     SlotGate s;
-    s.g = &g;
-    s.diag = is_diagonal(g);
-    for (int i = 0; i < g.nt; ++i) s.ts[i] = q2s[g.targets[i]];
-    s.nc = g.nc;
-    for (int i = 0; i < g.nc; ++i) s.cs[i] = q2s[g.controls[i]];
-    sgs.push_back(s);
+    s.rg = &r;
+    s.nt = 0;
+    if (r.kind == RK_FLUSH) {
+      s.diag = true;
+      for (int q : r.flq) s.slots.push_back(q2s[q]);
+    } else {
+      s.diag = r.kind == RK_MATRIX && is_diagonal(r.g);
+      for (int i = 0; i < r.g.nt; ++i) {
+        s.slots.push_back(q2s[r.g.targets[i]]);
+        if (!s.diag) s.ts[s.nt++] = q2s[r.g.targets[i]];
+      }
+      for (int i = 0; i < r.g.nc; ++i) s.slots.push_back(q2s[r.g.controls[i]]);
+    }
+    sgs.push_back(std::move(s));
   }
   auto low_union_size = [&](const std::vector<int>& t) {
     int extra = 0;
@@ -257,18 +593,22 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
     // ---- chunk: gates whose non-diagonal target slots (+ low slots) fit one tile
     std::vector<int> tset;
     size_t gend = gi;
-    int ops = 0, coefs = 0;
+    int ops = 0, coefs = 0, fls = 0;
     while (gend < sgs.size()) {
       std::vector<int> t2 = tset;
-      if (!sgs[gend].diag)
-        for (int i = 0; i < sgs[gend].g->nt; ++i)
-          if (std::find(t2.begin(), t2.end(), sgs[gend].ts[i]) == t2.end())
-            t2.push_back(sgs[gend].ts[i]);
+      for (int i = 0; i < sgs[gend].nt; ++i)
+        if (std::find(t2.begin(), t2.end(), sgs[gend].ts[i]) == t2.end())
+          t2.push_back(sgs[gend].ts[i]);
       const int cc = coef_count(sgs[gend]);
-      if (low_union_size(t2) > max_tile || ops + 1 > kMaxOps || coefs + cc > kMaxCoef) break;
+      const int nops_g = sgs[gend].rg->kind == RK_FLUSH ? 1 + int(sgs[gend].rg->flq.size()) : 1;
+      const int nfl_g = sgs[gend].rg->kind == RK_FLUSH ? int(sgs[gend].rg->flq.size()) : 0;
+      if (low_union_size(t2) > max_tile || ops + nops_g > kMaxOps || coefs + cc > kMaxCoef ||
+          fls + nfl_g > kMaxFlush)
+        break;
       tset = t2;
-      ++ops;
+      ops += nops_g;
       coefs += cc;
+      fls += nfl_g;
       ++gend;
     }
     if (gend == gi) return set_error(HS_E_INVALID, "gate does not fit a tile");
@@ -278,7 +618,7 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
     for (int s = 0; s < n && int(tile.size()) < m; ++s)
       if (std::find(tile.begin(), tile.end(), s) == tile.end()) tile.push_back(s);
     std::sort(tile.begin(), tile.end());
-    const int R = std::min(k1_reg_bits(dtype), m);
+    const int R = std::min(rbits, m);
     std::vector<int> tbit_of_slot(n, -1);
     for (int i = 0; i < m; ++i) tbit_of_slot[tile[i]] = i;
     PartProgram* P = nullptr;
@@ -308,27 +648,24 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       std::vector<int> regs;
       std::vector<size_t> members, rest;
       std::vector<int> blocked;  // slots held back by a deferred gate
-      auto touches = [&](const SlotGate& g, const std::vector<int>& set) {
-        for (int i = 0; i < g.g->nt; ++i)
-          if (std::find(set.begin(), set.end(), g.ts[i]) != set.end()) return true;
-        for (int i = 0; i < g.nc; ++i)
-          if (std::find(set.begin(), set.end(), g.cs[i]) != set.end()) return true;
+      auto touches = [&](const SlotGate& g) {
+        for (int s : g.slots)
+          if (std::find(blocked.begin(), blocked.end(), s) != blocked.end()) return true;
         return false;
       };
       auto block = [&](const SlotGate& g) {
-        for (int i = 0; i < g.g->nt; ++i) blocked.push_back(g.ts[i]);
-        for (int i = 0; i < g.nc; ++i) blocked.push_back(g.cs[i]);
+        for (int s : g.slots) blocked.push_back(s);
       };
       for (size_t x : remaining) {
         const SlotGate& g = sgs[x];
-        if (touches(g, blocked)) {
+        if (touches(g)) {
           block(g);
           rest.push_back(x);
           continue;
         }
         if (!g.diag) {
           std::vector<int> r2 = regs;
-          for (int i = 0; i < g.g->nt; ++i) {
+          for (int i = 0; i < g.nt; ++i) {
             const int tb = tbit_of_slot[g.ts[i]];
             if (std::find(r2.begin(), r2.end(), tb) == r2.end()) r2.push_back(tb);
           }
@@ -349,7 +686,10 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       for (int b = m - 1; b >= 0 && int(regs.size()) < R; --b)
         if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
       std::sort(regs.begin(), regs.end());
-      for (int j = 0; j < R; ++j) gd.reg_tbit[j] = uint8_t(regs[j]);
+      for (int j = 0; j < R; ++j) {
+        gd.reg_tbit[j] = uint8_t(regs[j]);
+        gd.dx[j] = smem_dx(regs[j], dtype);
+      }
       std::vector<int> thr;
       for (int b = 0; b < m; ++b)
         if (std::find(regs.begin(), regs.end(), b) == regs.end()) thr.push_back(b);
@@ -359,14 +699,30 @@ int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>
       for (int b = 0; b < kMaxTileBits; ++b) L.regpos_of_tbit[b] = -1;
       for (int j = 0; j < R; ++j) L.regpos_of_tbit[regs[j]] = j;
       gd.first_op = uint16_t(P->nops);
-      for (size_t x : members) emit_op(sgs[x], L, P);
+      Emitter E{P, &q2s};
+      for (size_t x : members) {
+        const SlotGate& sg = sgs[x];
+        if (sg.rg->kind == RK_ROT)
+          emit_rot(sg, L, E);
+        else if (sg.rg->kind == RK_FLUSH)
+          HS_TRY(emit_flush(sg, L, E));
+        else
+          emit_matrix(sg, L, E);
+      }
       gd.num_ops = uint16_t(P->nops - gd.first_op);
+      build_rounds(P, &gd);
       remaining = rest;
     }
     gi = gend;
   }
-  for (auto& P : *programs) factor_phases(&P);
   return HS_OK;
+}
+
+int plan_part(int n, const std::vector<int>& q2s, const std::vector<LoweredGate>& gates,
+              int tile_bits_hint, int dtype, std::vector<PartProgram>* programs) {
+  Frames fr;
+  fr.reset(n);
+  return plan_gates(n, q2s, gates, &fr, true, tile_bits_hint, dtype, programs);
 }
 
 }  // namespace hisv

@@ -54,9 +54,9 @@ def test_tile_hint_bounds():
     prev = abi.set_tile_qubits(11)
     assert abi.set_tile_qubits(prev) == 11
     assert abi.lib().hs_set_k1_reg_bits(2) == abi.HS_E_INVALID
-    prev = abi.set_k1_reg_bits(4)
-    assert prev == 3  # the default
-    assert abi.set_k1_reg_bits(prev) == 4
+    prev = abi.set_k1_reg_bits(3)
+    assert prev == 4  # the default
+    assert abi.set_k1_reg_bits(prev) == 3
 
 
 def test_fused_knob_bounds():
