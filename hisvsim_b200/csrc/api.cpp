@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <random>
+#include <set>
 
 #include "internal.h"
 
@@ -35,6 +36,31 @@ static std::mutex g_ev_mu;
 static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_events;
 static std::atomic<long long> g_apply_us{0};
 static std::atomic<int> g_timing{0};
+
+int device_sms() {
+  static std::mutex mu;
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lk(mu);
+  int& v = cache[dev & 63];
+  if (v <= 0 && (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                 v <= 0))
+    v = 148;
+  return v;
+}
+
+int smem_optin(const void* func) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  HS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, func})) return HS_OK;
+  HS_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  done.insert({dev, func});
+  return HS_OK;
+}
 
 void count_pass(long long gates) {
   g_passes += 1;

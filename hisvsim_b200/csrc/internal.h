@@ -332,6 +332,13 @@ int fp64_probe(double* tflops);
 int convert_kernel(const void* src, int sdtype, void* dst, int ddtype, uint64_t count,
                    cudaStream_t s);
 
+// ---- per-device launch facts ---------------------------------------------------
+// SM count of the current device (looked up once per device).
+int device_sms();
+// Raise the dynamic shared-memory limit of kernel `func` to 227 KiB on the
+// current device, once per (device, kernel); thread-safe.
+int smem_optin(const void* func);
+
 // ---- counters ---------------------------------------------------------------
 void count_pass(long long gates);
 // device-time accounting (hs_set_timing): brackets launches with CUDA events

@@ -1001,12 +1001,7 @@ int set_k4_variant(int v) { return g_k4_variant.exchange(v); }
 int launch_compose(const FusedGate* d_gates, const int32_t* d_offs, int nparts, double2* d_u,
                    void* d_a, cudaStream_t s) {
   if (nparts <= 0) return HS_OK;
-  static bool attr = false;
-  if (!attr) {
-    HS_CUDA(cudaFuncSetAttribute(k5_compose, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(double2) * kFusedDim * kFusedDim)));
-    attr = true;
-  }
+  HS_TRY(smem_optin(reinterpret_cast<const void*>(k5_compose)));
   k5_compose<<<nparts, kFusedDim, sizeof(double2) * kFusedDim * kFusedDim, s>>>(
       d_gates, d_offs, d_u, static_cast<uint8_t*>(d_a));
   HS_CUDA(cudaGetLastError());
@@ -1021,11 +1016,7 @@ int launch_pack(const double2* d_u, int nparts, void* d_a, cudaStream_t s) {
 }
 
 int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    HS_CUDA(cudaFuncSetAttribute(k4_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr = true;
-  }
+  HS_TRY(smem_optin(reinterpret_cast<const void*>(k4_fused)));
   const int T = 1 << P.m, N = T >> kFusedBits;
   const int variant = g_k4_variant.load();
   // the bulk form copies the lowest run of tile bits (slot 0 upward) and
@@ -1037,11 +1028,7 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
   if (bulk) {
     // A, four raw / B buffers, offset tables, sixteen mbarriers, the abort
     // word, the TMEM address and the epilogue's staging blocks
-    static bool battr = false;
-    if (!battr) {
-      HS_CUDA(cudaFuncSetAttribute(k4_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-      battr = true;
-    }
+    HS_TRY(smem_optin(reinterpret_cast<const void*>(k4_bulk)));
     const int chunk_bits = std::min<int>(P.tile.len[0], kBulkMaxChunkBits);
     const int nchunks = T >> chunk_bits;
     const int lgb = P.m <= 12 ? 2 : 1;  // ring of four buffers, or two for 2^13 tiles
@@ -1049,9 +1036,7 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
                          size_t(nchunks) * 8 + 64 * 4 + size_t(N) * 4 + 20 * 8 +
                          8 * kBulkStageFloats * 4;
     if (bsmem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 bulk pass needs %zu B", bsmem);
-    int bsms = 148, bdev = 0;
-    HS_CUDA(cudaGetDevice(&bdev));
-    HS_CUDA(cudaDeviceGetAttribute(&bsms, cudaDevAttrMultiProcessorCount, bdev));
+    const int bsms = device_sms();
     const int bgrid = int(P.ntiles < uint64_t(bsms) ? P.ntiles : uint64_t(bsms));
     k4_bulk<<<bgrid, kBulkThreads, bsmem, s>>>(static_cast<float2*>(amp), P,
                                                static_cast<const uint8_t*>(d_a), d_err, chunk_bits,
@@ -1061,17 +1046,11 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
   }
   if (P.nops == 1 && variant >= 1) {
     // warp-specialised form: A, two B buffers, offset tables, six mbarriers
-    static bool wattr = false;
-    if (!wattr) {
-      HS_CUDA(cudaFuncSetAttribute(k4_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-      wattr = true;
-    }
+    HS_TRY(smem_optin(reinterpret_cast<const void*>(k4_ws)));
     if (P.m > 13) return set_error(HS_E_UNSUPPORTED, "K4 tiles up to 2^13");
     const size_t wsmem = size_t(kFusedABytes) + size_t(N) * 1024 + 64 * 8 + size_t(N) * 8 +
                          6 * 8 + 8 + 16;
-    int wsms = 148, wdev = 0;
-    HS_CUDA(cudaGetDevice(&wdev));
-    HS_CUDA(cudaDeviceGetAttribute(&wsms, cudaDevAttrMultiProcessorCount, wdev));
+    const int wsms = device_sms();
     const int wgrid = int(P.ntiles < uint64_t(wsms) ? P.ntiles : uint64_t(wsms));
     k4_ws<<<wgrid, kWsThreads, wsmem, s>>>(static_cast<float2*>(amp), P,
                                            static_cast<const uint8_t*>(d_a), d_err);
@@ -1080,16 +1059,10 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
   }
   if (P.nops == 1) {
     // direct form: A, two B buffers, offset tables, barriers
-    static bool dattr = false;
-    if (!dattr) {
-      HS_CUDA(cudaFuncSetAttribute(k4_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-      dattr = true;
-    }
+    HS_TRY(smem_optin(reinterpret_cast<const void*>(k4_direct)));
     const size_t dsmem = size_t(kFusedABytes) + size_t(N) * 1024 + 64 * 8 + size_t(N) * 8 + 16 + 16;
     if (P.m > 13) return set_error(HS_E_UNSUPPORTED, "K4 tiles up to 2^13");
-    int dsms = 148, ddev = 0;
-    HS_CUDA(cudaGetDevice(&ddev));
-    HS_CUDA(cudaDeviceGetAttribute(&dsms, cudaDevAttrMultiProcessorCount, ddev));
+    const int dsms = device_sms();
     const int dgrid = int(P.ntiles < uint64_t(dsms) ? P.ntiles : uint64_t(dsms));
     k4_direct<<<dgrid, kK4DirectThreads, dsmem, s>>>(static_cast<float2*>(amp), P,
                                                static_cast<const uint8_t*>(d_a), d_err);
@@ -1102,10 +1075,8 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
   const size_t smem = size_t(P.nops) * kFusedABytes + size_t(N) * 512 + size_t(T) * 16 + tables +
                       8 * 8 + 8 + 8 + 16;
   if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 pass needs %zu B of shared memory", smem);
-  int sms = 148;
-  int dev = 0, per_sm = 1;
-  HS_CUDA(cudaGetDevice(&dev));
-  HS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int sms = device_sms();
+  int per_sm = 1;
   HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k4_fused, kK4Threads, smem));
   if (per_sm < 1) return set_error(HS_E_UNSUPPORTED, "K4 pass does not fit an SM");
   const uint64_t want = uint64_t(sms) * uint64_t(per_sm);

@@ -8,16 +8,7 @@
 namespace hisv {
 namespace {
 
-int num_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
-}
+int num_sms() { return device_sms(); }
 
 // ---- K2 -------------------------------------------------------------------
 // Replaces the MPI redistribution (gather_slots, mpi_redistributer.hpp:265-344)
@@ -441,11 +432,7 @@ int launch_tile_perm(V* amp, int n, const int32_t* pairs, int np, int max_bits, 
   const int T = 1 << P.m;
   const int per = T > kK2Threads ? T / kK2Threads : 1;
   const size_t smem = 2 * size_t(T) * sizeof(V) + size_t(per) * 8;
-  static bool attr = false;
-  if (!attr) {
-    HS_CUDA(cudaFuncSetAttribute(k2_tile<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-    attr = true;
-  }
+  HS_TRY(smem_optin(reinterpret_cast<const void*>(k2_tile<V>)));
   int per_sm = 1;
   HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2_tile<V>, kK2Threads, smem));
   const uint64_t want = uint64_t(num_sms()) * uint64_t(std::max(per_sm, 1));

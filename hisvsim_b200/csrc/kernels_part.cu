@@ -17,8 +17,6 @@
 // Op dispatch: every op carries one dense code (K1Code), so the switch below
 // is a jump table; op descriptors are read from the (warp-uniform) parameter
 // space, coefficients from a shared-memory copy (one 16-byte load each).
-#include <mutex>
-
 #include "internal.h"
 
 namespace hisv {
@@ -502,28 +500,9 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   cp_async_wait<0>();
 }
 
-// per-device launch facts: SM count and whether the shared-memory opt-in is set
-struct K1DeviceInfo {
-  int sms = 0;
-  bool attr = false;
-};
-
 template <int R, bool FULL, bool FAST, typename V>
 int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
-  static K1DeviceInfo info[64];
-  static std::mutex mu;
-  int dev = 0;
-  HS_CUDA(cudaGetDevice(&dev));
-  K1DeviceInfo& di = info[dev & 63];
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    if (!di.attr) {
-      HS_CUDA(cudaFuncSetAttribute(k1_part<R, FULL, FAST, V>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-      HS_CUDA(cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev));
-      di.attr = true;
-    }
-  }
+  HS_TRY(smem_optin(reinterpret_cast<const void*>(k1_part<R, FULL, FAST, V>)));
   const int threads = 1 << (P.m - R);
   const int per_thr = ((1 << P.m) * int(sizeof(V)) / 16) / threads;
   const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(double2) * P.ncoef +
@@ -533,7 +512,7 @@ int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
   int per_sm = 0;
   HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, FAST, V>, threads, smem));
   if (per_sm < 1) return set_error(HS_E_UNSUPPORTED, "K1 tile does not fit an SM (m=%d)", P.m);
-  const uint64_t want = uint64_t(di.sms) * uint64_t(per_sm);
+  const uint64_t want = uint64_t(device_sms()) * uint64_t(per_sm);
   const int grid = int(P.ntiles < want ? P.ntiles : want);
   k1_part<R, FULL, FAST, V><<<grid, threads, smem, s>>>(sv, P);
   HS_CUDA(cudaGetLastError());

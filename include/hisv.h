@@ -162,28 +162,32 @@ int hs_part_run(hs_state* st, const hs_gate* gates, int num_gates, void* stream)
 
 /* Several parts back to back (the loop of execute_qasm_parts,
  * qasm_assembler_standalone.py:1784-2018); part i is
- * gates[part_offsets[i] .. part_offsets[i+1]). */
+ * gates[part_offsets[i] .. part_offsets[i+1]).  One or more K1 passes per
+ * part; the phases that the factored one-qubit rotations leave pending are
+ * carried from part to part and applied by the last pass, so the state after
+ * the call is the reference's (to rounding) while the states between parts
+ * are not observable. */
 int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
                  int num_parts, void* stream);
 
-/* Host-only: plan one part (identity slot map) without touching a device and
- * report stats[0..5] = {passes, register groups, ops, dense ops, diagonal
- * ops, tile bits}.  Used by the cost model and by tests of the planner. */
 /* hs_parts_run with every part planned first and then launched back to back,
  * part_ms[p] = device time of part p (CUDA events between consecutive parts;
  * synchronises).  The harvest of part timings for the cost model. */
 int hs_parts_run_timed(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
                        int num_parts, float* part_ms, void* stream);
 
+/* Host-only: plan one part (identity slot map) without touching a device and
+ * report stats[0..5] = {passes, register groups, ops, dense ops, diagonal
+ * ops, tile bits}.  Used by the cost model and by tests of the planner. */
 int hs_plan_stats(int num_qubits, int dtype, const hs_gate* gates, int num_gates,
                   int32_t* stats);
 
 /* Tile-size override for K1 (0 = automatic).  Returns the previous value. */
 int hs_set_tile_qubits(int m);
-/* Amplitudes per thread of K1's complex128 passes: 2^r with r = 3 (default;
- * automatic tiles of 2^10 in CTAs of 128 threads, six per SM) or 4 (tiles of
- * 2^11 in CTAs of 128 threads, three per SM).  Complex64 passes always hold
- * 16.  Returns the previous value. */
+/* Amplitudes per thread of K1 passes: 2^r with r = 4 (default; complex128
+ * tiles of 2^10 in CTAs of 64 threads, or 2^11 in CTAs of 128) or 3 (CTAs
+ * twice as wide, register groups of three qubits).  Returns the previous
+ * value. */
 int hs_set_k1_reg_bits(int r);
 
 /* ---- precision form (complex64 state, fused unitaries on the tensor cores) --
@@ -196,11 +200,6 @@ int hs_set_k1_reg_bits(int r);
 #define HS_FUSED_BF16X1 1 /* one BF16 product (fast, ~2^-8) */
 int hs_fused_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
                        int num_parts, int precision, void* stream);
-/* K5 alone, for checking: the FP64 unitaries of the parts on an n-qubit
- * register with identity slot map.  out_u: num_parts x 64 x 64 complex128
- * (row-major, row = output basis index); out_qubits: num_parts x 6, the qubit
- * of each local bit (bit j = j-th lowest slot; parts smaller than six qubits
- * are padded with the lowest other qubits). */
 /* Apply one given 64x64 unitary (row-major, interleaved re/im doubles; local
  * index bit j = qubits[j]) to a complex64 state with K4: the form of
  * gather_and_execute_on for a part whose unitary the caller already has. */
@@ -218,6 +217,11 @@ int hs_set_k4_variant(int variant);
  * 1 with 10..13 (default 1, 13) or 2 with 10..12.  Returns the previous
  * shape as ops * 100 + bits. */
 int hs_set_fused_shape(int max_ops_per_pass, int tile_bits);
+/* K5 alone, for checking: the FP64 unitaries of the parts on an n-qubit
+ * register with identity slot map.  out_u: num_parts x 64 x 64 complex128
+ * (row-major, row = output basis index); out_qubits: num_parts x 6, the qubit
+ * of each local bit (bit j = j-th lowest slot; parts smaller than six qubits
+ * are padded with the lowest other qubits). */
 int hs_fused_compose(int num_qubits, const hs_gate* gates, const int32_t* part_offsets,
                      int num_parts, double* out_u, int32_t* out_qubits);
 /* out = {Re<a|b>, Im<a|b>, max|a-b|, <b|b>} in FP64 for states of any two

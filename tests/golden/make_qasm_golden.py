@@ -21,7 +21,9 @@ import sys
 from datetime import datetime
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HISV_REFERENCE")
+       or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                       "reference"))
 SRC = os.path.join(REF, "qasm_assembler_standalone.py")
 
 PARAM_CASES = ["0.5", "-0.75", "3", "1e-3", "0.25e1", "pi", "-pi", "pi/2", "-pi/2", "pi/8",
