@@ -146,6 +146,12 @@ struct PartProgram {
   Runs tile;           // tile index -> global index
   Runs outer;          // tile number -> global index
   uint8_t tile_slot[16];  // global slot of tile bit b
+  // shared-memory layout of the tile: 16-byte slot s (tile index >> SH, SH =
+  // 1 for complex64) sits at slot s ^ (XOR over the set bits k of s of
+  // fold[k]); fold[k] < 8 only moves a slot within its 128-byte row.  The
+  // planner picks fold per program so that the lanes of every register
+  // group's shared-memory accesses hit distinct banks.
+  uint8_t fold[16];
   int32_t nfl;         // used entries of flw / flp
   uint8_t flw[kMaxFlush], flp[kMaxFlush];  // flush entries: where (TW_THR / TW_OUT), position
   int32_t nrounds, nothers;

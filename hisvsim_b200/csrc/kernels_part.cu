@@ -75,12 +75,14 @@ __device__ __forceinline__ uint64_t deposit(uint64_t x, const Runs& r) {
   return out;
 }
 
-// shared-memory slot of tile index i: XOR the 16-byte slot within a 128-byte
-// row with a fold of the higher bits, so that lanes differing in any three
-// bits with distinct residues mod 3 hit distinct bank groups (the planner
-// computes the same function for the per-group offsets)
-__device__ __forceinline__ uint32_t swz(uint32_t i) {
-  return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9) ^ (i >> 12)) & 7u);
+// shared-memory slot of 16-byte slot s: s XOR the program's fold of its bits
+// (a move within the 128-byte row, chosen by the planner so that every
+// register group's lanes hit distinct banks)
+__device__ __forceinline__ uint32_t swz(const PartProgram& P, uint32_t s) {
+  uint32_t r = s;
+  for (int k = 0; s >> k; ++k)
+    if ((s >> k) & 1u) r ^= P.fold[k];
+  return r;
 }
 
 // ---- gate bodies on registers (in place) -------------------------------------
@@ -335,52 +337,52 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // Shared-memory byte offset of tile index i: 16-byte slots hold 1 (complex128)
-// or 2 (complex64) amplitudes; slots are XOR-swizzled (swz is linear over
-// GF(2), so the offset of thr | reg(e) is built from per-bit parts).
+// or 2 (complex64) amplitudes; slots are moved by the program's fold (linear
+// over GF(2), so the offset of thr | reg(e) is built from per-bit parts).
 template <typename V>
 struct SmemMap {
   static constexpr int SH = sizeof(V) == 8 ? 1 : 0;  // amplitudes per slot = 2^SH
-  __device__ __forceinline__ static uint32_t off(uint32_t i) {
-    return (swz(i >> SH) << 4) | ((i & ((1u << SH) - 1u)) * uint32_t(sizeof(V)));
+  __device__ __forceinline__ static uint32_t off(const PartProgram& P, uint32_t i) {
+    return (swz(P, i >> SH) << 4) | ((i & ((1u << SH) - 1u)) * uint32_t(sizeof(V)));
   }
 };
 
-// Issue the asynchronous copy of one tile into a shared buffer: 16-byte
-// chunks, chunk c covering tile indices [c*2^SH, (c+1)*2^SH) that are
-// contiguous in global memory (tile bit 0 is always global slot 0 when SH=1).
+// Issue the asynchronous copy of one tile into the shared buffer: 16-byte
+// chunks, chunk c = t + k*nthr covering tile indices [c*2^SH, (c+1)*2^SH)
+// that are contiguous in global memory (tile bit 0 is always global slot 0
+// when SH=1); its shared slot is swz(t) ^ swz(k*nthr) (disjoint bits).
 template <typename V>
 __device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32_t sbuf,
                                                 uint64_t gbase, const uint64_t* __restrict__ gchunk,
+                                                const uint32_t* __restrict__ cswz, uint32_t tswz,
                                                 uint64_t gt, int nchunk_per_thr) {
-  const uint32_t t = threadIdx.x;
   const V* base = sv + gbase + gt;
-  for (int k = 0; k < nchunk_per_thr; ++k) {
-    const uint32_t c = t + uint32_t(k) * blockDim.x;
-    cp_async16(sbuf + (swz(c) << 4), base + gchunk[k]);
-  }
+  for (int k = 0; k < nchunk_per_thr; ++k) cp_async16(sbuf + (tswz ^ cswz[k]), base + gchunk[k]);
 }
 
 // CTA shapes: 2^(m-R) threads.  Complex128 with 16 amplitudes per thread:
-// 2^10 tiles in CTAs of 64 threads (six per SM, by shared memory) or 2^11
-// tiles in CTAs of 128 (three per SM); the register bound leaves room for
-// three CTAs of 128.  8 amplitudes per thread (R = 3): up to 256 threads.
+// 2^10 tiles in CTAs of 64 threads or 2^11 tiles in CTAs of 128, one tile
+// buffer each.  8 amplitudes per thread (R = 3): up to 256 threads.
 // Complex64: 2^12 tiles, 256 threads.
 constexpr int kThrCache = 8;  // groups whose thread parts are tabulated per launch
 
-template <typename V, int R, bool FULL>
+template <typename V, int R, bool FULL, bool FAST>
 struct K1Threads {
   static constexpr int value = 256;
-  // complex64 with 4x4 ops on 16 amplitudes: room for the coefficient loads
-  static constexpr int min_blocks = (R >= 4 && FULL) ? 1 : 2;
+  // complex64 with 4x4 ops: room for the coefficient loads
+  static constexpr int min_blocks = (R >= 3 && FULL) ? 1 : 2;
 };
-template <int R, bool FULL>
-struct K1Threads<double2, R, FULL> {
+// complex128, 16 amplitudes per thread: the frequent-op instantiation is held
+// to ~100 registers so that five CTAs of 128 (ten of 64) share an SM; the
+// general ones get ~168
+template <int R, bool FULL, bool FAST>
+struct K1Threads<double2, R, FULL, FAST> {
   static constexpr int value = R >= 4 ? 128 : 256;
-  static constexpr int min_blocks = R >= 4 ? 3 : 2;
+  static constexpr int min_blocks = R >= 4 ? (FAST ? 5 : 3) : 2;
 };
 
 template <int R, bool FULL, bool FAST, typename V>
-__global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, FULL>::min_blocks)
+__global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<V, R, FULL, FAST>::min_blocks)
     k1_part(V* __restrict__ sv, const __grid_constant__ PartProgram P) {
   using M = SmemMap<V>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   const uint32_t t = threadIdx.x;
   const uint32_t nthr = blockDim.x;
   const uint32_t tile_bytes = uint32_t(sizeof(V)) << P.m;
-  double2* s_coef = reinterpret_cast<double2*>(smem_raw + 2 * tile_bytes);
+  double2* s_coef = reinterpret_cast<double2*>(smem_raw + tile_bytes);
   uint64_t* s_gchunk = reinterpret_cast<uint64_t*>(s_coef + P.ncoef);
   // chunk c = t + k*nthr; its first tile index is c << SH.  The bits of t and
   // of k*nthr are disjoint, so deposit(c << SH) = deposit(t << SH) + deposit(k*nthr << SH).
@@ -399,39 +401,39 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
   uint64_t* s_glreg = s_gchunk + per_thr;
   uint64_t* s_glthr = s_glreg + R;
   // the thread part (tile index bits held by this thread) of the first
-  // kThrCache groups, the same in every tile
+  // kThrCache groups and its shared-memory offset, the same in every tile
   uint32_t* s_thr = reinterpret_cast<uint32_t*>(s_glthr + nthr);
+  uint32_t* s_a0 = s_thr + kThrCache * nthr;
+  // shared slot part of chunk k*nthr (the copy of a tile)
+  uint32_t* s_cswz = s_a0 + kThrCache * nthr;
   const GroupDesc& GL = P.groups[P.ngroups - 1];
   for (int i = int(t); i < P.ncoef; i += int(nthr)) s_coef[i] = P.coef[i];
-  for (int k = int(t); k < per_thr; k += int(nthr))
+  for (int k = int(t); k < per_thr; k += int(nthr)) {
     s_gchunk[k] = deposit(uint64_t(k) * nthr << M::SH, P.tile);
+    s_cswz[k] = swz(P, uint32_t(k) * nthr) << 4;
+  }
   for (int j = int(t); j < R; j += int(nthr)) s_glreg[j] = deposit(1ull << GL.reg_tbit[j], P.tile);
   // (the last group's lanes run over the lowest free tile bits, so the direct
   // stores coalesce)
   s_glthr[t] = deposit(deposit(t, GL.thr), P.tile);
-  for (int g = 0; g < P.ngroups && g < kThrCache; ++g)
-    s_thr[g * nthr + t] = uint32_t(deposit(t, P.groups[g].thr));
+  for (int g = 0; g < P.ngroups && g < kThrCache; ++g) {
+    const uint32_t thr = uint32_t(deposit(t, P.groups[g].thr));
+    s_thr[g * nthr + t] = thr;
+    s_a0[g * nthr + t] = M::off(P, thr);
+  }
+  const uint32_t tswz = swz(P, t) << 4;
   __syncthreads();
   const uint64_t gt = deposit(uint64_t(t) << M::SH, P.tile);
   const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(smem_raw));
-  const uint32_t sb1 = sb0 + tile_bytes;
 
   uint64_t tile = blockIdx.x;
-  if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, deposit(tile, P.outer), s_gchunk, gt, per_thr);
+  if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, deposit(tile, P.outer), s_gchunk, s_cswz, tswz, gt, per_thr);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
   V v[E];
-  for (int it = 0; tile < P.ntiles; ++it, tile += gridDim.x) {
-    // this tile has landed and every thread is past the previous one (the
-    // barrier that ends the previous tile's last group), so the previous
-    // tile's buffer may take the next tile
+  for (; tile < P.ntiles; tile += gridDim.x) {
     const uint64_t next = tile + gridDim.x;
-    if (next < P.ntiles) {
-      issue_tile_load<V>(sv, (it & 1) ? sb0 : sb1, deposit(next, P.outer), s_gchunk, gt, per_thr);
-      cp_async_commit();
-    }
-    const uint32_t boff = (it & 1) ? tile_bytes : 0u;
     const uint64_t gbase = deposit(tile, P.outer);
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
@@ -439,7 +441,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
       const uint32_t thr = g < kThrCache ? s_thr[g * nthr + t] : uint32_t(deposit(t, G.thr));
       // offset of element e: the thread's slot XOR the (warp-uniform) change
       // of e's register bits, whose per-bit parts come from the planner
-      const uint32_t a0 = M::off(thr);
+      const uint32_t a0 = g < kThrCache ? s_a0[g * nthr + t] : M::off(P, thr);
       auto ux = [&](int e) {
         uint32_t d = 0;
 #pragma unroll
@@ -448,8 +450,17 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
         return d;
       };
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-        v[e] = *reinterpret_cast<const V*>(smem_raw + boff + (a0 ^ ux(e)));
+      for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(smem_raw + (a0 ^ ux(e)));
+      if (last) {
+        // every thread holds its registers of the last group: the buffer
+        // takes the next tile while this one is finished and stored (one
+        // tile buffer per CTA leaves room for more CTAs per SM)
+        __syncthreads();
+        if (next < P.ntiles) {
+          issue_tile_load<V>(sv, sb0, deposit(next, P.outer), s_gchunk, s_cswz, tswz, gt, per_thr);
+          cp_async_commit();
+        }
+      }
       // the group's rounds: one rotation per register bit in a fixed order
       // (uniform tests, no dispatch), then the round's other ops
       Deferred dfr;
@@ -488,11 +499,10 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL>::value, K1Threads<V, R, 
           __stcs(p, v[e]);
         }
         // the next tile's copies (the only ones in flight) must have landed
-        // and every thread must be done with this tile's buffer
         cp_async_wait<0>();
       } else {
 #pragma unroll
-        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(smem_raw + boff + (a0 ^ ux(e))) = v[e];
+        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(smem_raw + (a0 ^ ux(e))) = v[e];
       }
       __syncthreads();
     }
@@ -505,9 +515,9 @@ int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
   HS_TRY(smem_optin(reinterpret_cast<const void*>(k1_part<R, FULL, FAST, V>)));
   const int threads = 1 << (P.m - R);
   const int per_thr = ((1 << P.m) * int(sizeof(V)) / 16) / threads;
-  const size_t smem = 2 * (sizeof(V) << P.m) + sizeof(double2) * P.ncoef +
+  const size_t smem = (sizeof(V) << P.m) + sizeof(double2) * P.ncoef +
                       sizeof(uint64_t) * (per_thr + R + threads) +
-                      sizeof(uint32_t) * kThrCache * threads;
+                      sizeof(uint32_t) * (2 * kThrCache * threads + per_thr);
   if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K1 tile of 2^%d needs %zu B", P.m, smem);
   int per_sm = 0;
   HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, FAST, V>, threads, smem));

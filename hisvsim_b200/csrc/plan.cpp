@@ -38,6 +38,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <functional>
 
 #include "internal.h"
 
@@ -521,13 +522,111 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
   gd->num_rounds = uint16_t(P->nrounds - gd->first_round);
 }
 
-// XOR-swizzled shared-memory slot (the same function as the kernel's)
-uint32_t swz(uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9) ^ (i >> 12)) & 7u); }
+// ---- shared-memory layout ----------------------------------------------------
+// Slot s of the tile (16 bytes) sits at s ^ fold(s), fold(s) = XOR over the
+// set bits k of s of fold[k] (3 bits: a move within the 128-byte row).
+uint32_t fold_of(const PartProgram& P, uint32_t s) {
+  uint32_t r = 0;
+  for (int k = 0; k < 16; ++k)
+    if ((s >> k) & 1u) r ^= P.fold[k];
+  return r;
+}
 
-uint32_t smem_dx(int tbit, int dtype) {
+// Byte offset change of setting tile bit tbit (the map is linear over GF(2)).
+uint32_t smem_dx(const PartProgram& P, int tbit, int dtype) {
   const int sh = dtype == HS_DTYPE_C64 ? 1 : 0;
   const uint32_t b = 1u << tbit;
-  return (swz(b >> sh) << 4) ^ ((b & ((1u << sh) - 1u)) * uint32_t(amp_bytes(dtype)));
+  const uint32_t slot = b >> sh;
+  return ((slot ^ fold_of(P, slot)) << 4) ^ ((b & ((1u << sh) - 1u)) * uint32_t(amp_bytes(dtype)));
+}
+
+// Pick fold so that, in every register group, the lanes of one access phase
+// (8 lanes of 16 bytes for complex128, 16 of 8 bytes for complex64) hit
+// distinct banks: the lanes differ in the group's lowest thread tile bits,
+// whose images (slot bits 0..2 after the fold, plus the in-slot bit for
+// complex64) must be linearly independent.  Slot bits 0..2 keep fold 0, so
+// the chunked tile copy (lanes over consecutive slots) is conflict-free too.
+// Small backtracking search, the fixed fold of the earlier layout (bit k >= 3
+// onto bit k mod 3) first; kept when no assignment is found.
+void choose_fold(PartProgram* P, int dtype) {
+  const int sh = dtype == HS_DTYPE_C64 ? 1 : 0;
+  const int nslot = P->m - sh;
+  const int lane_bits = std::min(dtype == HS_DTYPE_C64 ? 4 : 3, P->m - P->rbits);
+  std::memset(P->fold, 0, sizeof(P->fold));
+  for (int k = 3; k < nslot; ++k) P->fold[k] = uint8_t(1u << (k % 3));
+  if (lane_bits < 1 || nslot <= 3) return;
+  // constraints: the lane tile bits of each group
+  std::vector<std::vector<int>> cons;
+  for (int g = 0; g < P->ngroups; ++g) {
+    std::vector<int> lb;
+    for (int b = 0; b < P->m && int(lb.size()) < lane_bits; ++b) {
+      bool reg = false;
+      for (int j = 0; j < P->rbits; ++j) reg |= P->groups[g].reg_tbit[j] == b;
+      if (!reg) lb.push_back(b);
+    }
+    cons.push_back(lb);
+  }
+  auto vec = [&](const uint8_t* F, int tbit) -> uint32_t {
+    if (tbit < sh) return 8u << tbit;  // in-slot bit: its own dimension
+    const int k = tbit - sh;
+    return (k < 3 ? (1u << k) : 0u) ^ F[k];
+  };
+  // the lanes' images must have full rank: min(lanes, 3 slot bits + the
+  // in-slot bit when a lane bit is one) -- complex64 lanes that share the
+  // in-slot half can at best hit every bank pair twice
+  auto independent = [&](const uint8_t* F, const std::vector<int>& lb) {
+    int dims = 3;
+    for (int b : lb) dims += b < sh;
+    const int want = std::min(int(lb.size()), dims);
+    uint32_t basis[8];
+    int rank = 0;
+    for (int b : lb) {
+      uint32_t x = vec(F, b);
+      for (int i = 0; i < rank; ++i) x = std::min(x, x ^ basis[i]);
+      if (x) basis[rank++] = x;
+      for (int i = rank - 1; i > 0 && basis[i] > basis[i - 1]; --i) std::swap(basis[i], basis[i - 1]);
+    }
+    return rank >= want;
+  };
+  // the highest slot bit each constraint involves (checked once it is set)
+  auto top = [&](const std::vector<int>& lb) {
+    int t = -1;
+    for (int b : lb) t = std::max(t, b - sh);
+    return t;
+  };
+  uint8_t F[16];
+  std::memcpy(F, P->fold, sizeof(F));
+  bool ok = true;
+  for (const auto& c : cons)
+    if (!independent(F, c)) ok = false;
+  if (ok) return;
+  int budget = 20000;
+  std::function<bool(int)> dfs = [&](int k) -> bool {
+    if (--budget < 0) return false;
+    if (k >= nslot) return true;
+    const uint8_t first = uint8_t(1u << (k % 3));
+    for (int i = 0; i < 8; ++i) {
+      const uint8_t cand = uint8_t(i == 0 ? first : (i == first ? 0 : i));
+      F[k] = cand;
+      bool good = true;
+      for (const auto& c : cons)
+        if (top(c) == k && !independent(F, c)) {
+          good = false;
+          break;
+        }
+      if (good && dfs(k + 1)) return true;
+    }
+    F[k] = first;
+    return false;
+  };
+  // constraints that involve only slot bits 0..2 do not depend on fold
+  if (dfs(3)) std::memcpy(P->fold, F, sizeof(F));
+}
+
+void finish_layout(PartProgram* P, int dtype) {
+  choose_fold(P, dtype);
+  for (int g = 0; g < P->ngroups; ++g)
+    for (int j = 0; j < P->rbits; ++j) P->groups[g].dx[j] = smem_dx(*P, P->groups[g].reg_tbit[j], dtype);
 }
 
 }  // namespace
@@ -686,10 +785,7 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
       for (int b = m - 1; b >= 0 && int(regs.size()) < R; --b)
         if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
       std::sort(regs.begin(), regs.end());
-      for (int j = 0; j < R; ++j) {
-        gd.reg_tbit[j] = uint8_t(regs[j]);
-        gd.dx[j] = smem_dx(regs[j], dtype);
-      }
+      for (int j = 0; j < R; ++j) gd.reg_tbit[j] = uint8_t(regs[j]);
       std::vector<int> thr;
       for (int b = 0; b < m; ++b)
         if (std::find(regs.begin(), regs.end(), b) == regs.end()) thr.push_back(b);
@@ -715,6 +811,7 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
     }
     gi = gend;
   }
+  for (auto& P : *programs) finish_layout(&P, dtype);
   return HS_OK;
 }
 

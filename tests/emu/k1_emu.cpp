@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "internal.h"
@@ -42,7 +43,12 @@ uint64_t deposit(uint64_t x, const Runs& r) {
   for (int i = 0; i < r.n; ++i) out |= ((x >> r.src[i]) & ((1ull << r.len[i]) - 1ull)) << r.dst[i];
   return out;
 }
-uint32_t swz(uint32_t i) { return i ^ (((i >> 3) ^ (i >> 6) ^ (i >> 9) ^ (i >> 12)) & 7u); }
+uint32_t swz(const PartProgram& P, uint32_t s) {
+  uint32_t r = s;
+  for (int k = 0; (s >> k) != 0; ++k)
+    if ((s >> k) & 1u) r ^= P.fold[k];
+  return r;
+}
 int lowest_bit(int e) { return __builtin_ctz(unsigned(e)); }
 C cc(const double2& d) { return C(d.x, d.y); }
 
@@ -51,7 +57,7 @@ struct Emu {
   int R, E, SH, ab;
   std::vector<unsigned char> buf;
   uint32_t off(uint32_t i) const {
-    return (swz(i >> SH) << 4) | ((i & ((1u << SH) - 1u)) * uint32_t(ab));
+    return (swz(P, i >> SH) << 4) | ((i & ((1u << SH) - 1u)) * uint32_t(ab));
   }
   C ld(uint32_t o) const {
     if (ab == 16) {
@@ -176,6 +182,8 @@ void run_op(std::vector<C>& v, int R, const PartProgram& P, const DevOp& op, con
   for (int e = 0; e < E; ++e) v[e] = rnd(v[e], ab);
 }
 
+int64_t wave_total = 0, wave_ideal = 0;
+
 void run_program(const PartProgram& P, int ab, std::vector<C>& sv) {
   const int R = P.rbits, E = 1 << R, m = P.m;
   const int nthr = 1 << (m - R);
@@ -198,9 +206,29 @@ void run_program(const PartProgram& P, int ab, std::vector<C>& sv) {
       for (int k = 0; k < per_thr; ++k) {
         const uint32_t cix = uint32_t(t + k * nthr);
         const uint64_t g = gbase + gt + gchunk[k];
-        for (int s = 0; s < (1 << SH); ++s) em.st((swz(cix) << 4) + s * ab, sv[g + s]);
+        for (int s = 0; s < (1 << SH); ++s) em.st((swz(P, cix) << 4) + s * ab, sv[g + s]);
       }
     }
+    if (tile == 0)
+      for (int g = 0; g < P.ngroups; ++g) {
+        const GroupDesc& G = P.groups[g];
+        const int plen = ab == 16 ? 8 : 16;
+        for (int t0 = 0; t0 < nthr; t0 += plen) {
+          int cnt[16] = {0};
+          int worst = 0;
+          uint32_t halves = 0;
+          for (int t = t0; t < t0 + plen && t < nthr; ++t) {
+            const uint32_t a = em.off(uint32_t(deposit(t, G.thr)));
+            const int key = ab == 16 ? int((a >> 4) & 7u) : int((a >> 3) & 15u);
+            worst = std::max(worst, ++cnt[key]);
+            halves |= 1u << ((a >> 3) & 1u);
+          }
+          wave_total += worst;
+          // lower bound: 8-byte lanes that all sit in the same half of their
+          // 16-byte slots reach only 8 distinct bank pairs
+          wave_ideal += (ab == 8 && halves != 3u) ? 2 : 1;
+        }
+      }
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
       const bool last = g == P.ngroups - 1;
@@ -260,7 +288,8 @@ const char* emu_last_error() { return g_err; }
 // per_part != 0 every part is planned on its own and flushed) and execute on
 // `amps` (2^n interleaved complex128, in/out).  dtype HS_DTYPE_C64 rounds the
 // amplitudes to complex64 as the kernel would.  stats: {passes, groups, ops,
-// rotation ops, max tile bits, rounds}.
+// rotation ops, max tile bits, rounds, shared-memory wavefronts of the group
+// loads of one tile (summed over programs), the conflict-free count}.
 int emu_parts_run(int n, int dtype, const hs_gate* gates, const int32_t* offs, int nparts,
                   int rbits, int tile_hint, int per_part, double* amps, int32_t* stats) {
   g_rbits = rbits;
@@ -270,7 +299,8 @@ int emu_parts_run(int n, int dtype, const hs_gate* gates, const int32_t* offs, i
   for (int q = 0; q < n; ++q) q2s[q] = q;
   Frames fr;
   fr.reset(n);
-  int32_t st[6] = {0, 0, 0, 0, 0, 0};
+  int32_t st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  wave_total = wave_ideal = 0;
   for (int p = 0; p < nparts; ++p) {
     std::vector<LoweredGate> lg(offs[p + 1] - offs[p]);
     for (int i = offs[p]; i < offs[p + 1]; ++i) {
@@ -296,6 +326,8 @@ int emu_parts_run(int n, int dtype, const hs_gate* gates, const int32_t* offs, i
     amps[2 * i] = sv[i].real();
     amps[2 * i + 1] = sv[i].imag();
   }
+  st[6] = int32_t(wave_total);
+  st[7] = int32_t(wave_ideal);
   if (stats) std::memcpy(stats, st, sizeof(st));
   return HS_OK;
 }

@@ -43,13 +43,13 @@ def emu(tmp_path_factory):
             a[0] = 1
         else:
             a[:] = init
-        st = np.zeros(6, np.int32)
+        st = np.zeros(8, np.int32)
         rc = lib.emu_parts_run(n, dtype, rec.ctypes.data, offs.ctypes.data, len(offs) - 1, rbits,
                                hint, int(per_part), a.ctypes.data, st.ctypes.data)
         if rc:
             raise RuntimeError(lib.emu_last_error().decode())
-        return a, dict(zip(["passes", "groups", "ops", "rotations", "tile_bits", "rounds"],
-                           st.tolist()))
+        return a, dict(zip(["passes", "groups", "ops", "rotations", "tile_bits", "rounds",
+                            "wavefronts", "wavefronts_ideal"], st.tolist()))
     return run
 
 
@@ -126,3 +126,14 @@ def test_every_gate_kind_with_frames(emu, port):
         for per_part in (False, True):
             got, _ = emu(n, rec, offs, per_part=per_part)
             assert np.abs(got - want).max() <= 1e-12 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.parametrize("dtype", [0, 1])
+def test_group_loads_are_conflict_free(emu, dtype):
+    """The per-program shared-memory fold puts the lanes of every register
+    group's loads on distinct banks (U3 + CZ layers, parts of <= 9 qubits)."""
+    gates = circuits.random_u3_cz(16, 12, 2)
+    parts = partition.partition_dfs(gates, 9)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    _, st = emu(16, rec, offs, dtype=dtype)
+    assert st["wavefronts"] == st["wavefronts_ideal"]
