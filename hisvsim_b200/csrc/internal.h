@@ -114,18 +114,24 @@ struct Runs {  // bit-run deposit: out |= ((x >> src) & (2^len - 1)) << dst
   uint8_t dst[kMaxRuns];
 };
 
-// A round of a register group: at most one rotation per register bit j (bit
-// j of `mask`; with an RZ part when bit j of `zmask` is set; coefficients at
-// coef[cidx[j]]), applied in the order j = 0, 1, ..., then the ops
-// ops[first_other, first_other + num_other).  The planner packs a group's ops
-// into rounds without changing their order where they do not commute.
-struct RoundDesc {
-  uint8_t mask, zmask;
-  uint16_t first_other, num_other;
-  uint16_t cidx[kRegBits];
-  uint16_t pad;
-};
-static_assert(sizeof(RoundDesc) == 16, "RoundDesc layout");
+// A round of a register group, packed in one 64-bit word (read with a single
+// load): at most one rotation per register bit j, applied in the order
+// j = 0, 1, ..., then ops[others[first_other .. first_other + num_other)).
+//   bits  0- 3  rotation on register bit j present
+//   bits  4- 7  with a phase part
+//   bits  8-15  num_other
+//   bits 16-23  first_other
+//   bits 24+10j coefficient index of the rotation on bit j (coef[idx], [idx+1])
+// The planner packs a group's ops into rounds without changing their order
+// where they do not commute.
+using RoundDesc = uint64_t;
+inline RoundDesc round_pack(uint32_t mask, uint32_t zmask, uint32_t first_other,
+                            uint32_t num_other, const uint32_t cidx[4]) {
+  uint64_t w = uint64_t(mask & 15u) | uint64_t(zmask & 15u) << 4 | uint64_t(num_other & 255u) << 8 |
+               uint64_t(first_other & 255u) << 16;
+  for (int j = 0; j < 4; ++j) w |= uint64_t(cidx[j] & 1023u) << (24 + 10 * j);
+  return w;
+}
 
 struct GroupDesc {
   uint8_t reg_tbit[kRegBits];  // tile bit held by register bit j
@@ -157,11 +163,12 @@ struct PartProgram {
   int32_t nrounds, nothers;
   GroupDesc groups[kMaxGroups];
   DevOp ops[kMaxOps];            // per group: rotations and others in program order
-  uint16_t others[kMaxOps];      // per round: indices into ops of its non-rotation ops
+  uint8_t others[kMaxOps];       // per round: indices into ops of its non-rotation ops
   RoundDesc rounds[kMaxRounds];
   double2 coef[kMaxCoef];
 };
 static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
+static_assert(kMaxOps <= 256 && kMaxCoef <= 1024, "round packing");
 
 // Pending diagonal of a state under planning: the true state is
 // G * (prod_q diag(1, r[q]) on qubit q) * (the stored amplitudes).  Uncontrolled
@@ -194,9 +201,11 @@ int current_tile_hint();  // hs_set_tile_qubits' value
 // register bits per thread of K1 programs (hs_set_k1_reg_bits: 4 = 16
 // amplitudes (default), 3 = 8 amplitudes)
 int k1_reg_bits(int dtype);
-// complex128 tiles stop at 2^11 (two 32 KiB buffers per CTA); complex64
-// tiles go to 2^12
-inline int max_tile_bits(int dtype) { return dtype == HS_DTYPE_C64 ? 12 : 11; }
+// tiles go to 2^12 amplitudes (one 64 KiB buffer per CTA for complex128);
+// complex128 with 8 amplitudes per thread stops at 2^11 (256 threads)
+inline int max_tile_bits(int dtype) {
+  return dtype == HS_DTYPE_C64 ? 12 : (k1_reg_bits(dtype) >= 4 ? 12 : 11);
+}
 
 // ---- K2 bit-swap program ----------------------------------------------------
 struct PermProgram {

@@ -257,16 +257,20 @@ __device__ __forceinline__ void apply_deferred(V (&v)[1 << R], const Deferred& d
 // cases at its join (measured: ~50 register moves per op and 160 instead of
 // ~110 registers per thread).
 template <int R, bool FULL, bool FAST, typename V>
-__device__ __forceinline__ void run_op(V (&v)[1 << R], const DevOp& op, const double2* c,
+__device__ __forceinline__ void run_op(V (&v)[1 << R], const DevOp& op, const double2* s_coef,
                                        uint32_t thr, uint64_t gbase, Deferred& dfr,
                                        const PartProgram& P) {
   constexpr int E = 1 << R;
-  const int code = op.code;
+  // the op's first 24 bytes in three 8-byte loads: code (byte 1), coefficient
+  // index (bytes 8-9), thread mask (bytes 12-15), outer mask (bytes 16-23)
+  const uint64_t* ow = reinterpret_cast<const uint64_t*>(&op);
+  const uint64_t w0 = ow[0], w1 = ow[1], w2 = ow[2];
+  const int code = int(w0 >> 8) & 255;
+  const double2* c = s_coef + (uint32_t(w1) & 0xffffu);
+  const uint32_t cthr = uint32_t(w1 >> 32);
   // thread and outer part of the controls (the register part is in the code /
   // creg); evaluated only by the ops that have such controls
-  auto ok = [&]() {
-    return ((thr & op.cthr) == op.cthr) && ((gbase & op.couter) == op.couter);
-  };
+  auto ok = [&]() { return ((thr & cthr) == cthr) && ((gbase & w2) == w2); };
   if (code >= kc_neg && code < kc_ph) {  // sign flips (CZ and other -1 phases)
     const uint32_t sm = ok() ? 0x80000000u : 0u;
 #define NEG(M) \
@@ -366,23 +370,23 @@ __device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32
 // Complex64: 2^12 tiles, 256 threads.
 constexpr int kThrCache = 8;  // groups whose thread parts are tabulated per launch
 
-template <typename V, int R, bool FULL, bool FAST>
+template <typename V, int R, bool FULL, bool FAST, bool WIDE>
 struct K1Threads {
   static constexpr int value = 256;
   // complex64 with 4x4 ops: room for the coefficient loads
   static constexpr int min_blocks = (R >= 3 && FULL) ? 1 : 2;
 };
 // complex128, 16 amplitudes per thread: the frequent-op instantiation is held
-// to ~100 registers so that five CTAs of 128 (ten of 64) share an SM; the
-// general ones get ~168
-template <int R, bool FULL, bool FAST>
-struct K1Threads<double2, R, FULL, FAST> {
-  static constexpr int value = R >= 4 ? 128 : 256;
-  static constexpr int min_blocks = R >= 4 ? (FAST ? 5 : 3) : 2;
+// to ~100 registers so that five CTAs of 128 (ten of 64) share an SM, the
+// general ones get ~168; WIDE (2^12 tiles, 256 threads) is held to 128
+template <int R, bool FULL, bool FAST, bool WIDE>
+struct K1Threads<double2, R, FULL, FAST, WIDE> {
+  static constexpr int value = (WIDE || R < 4) ? 256 : 128;
+  static constexpr int min_blocks = WIDE ? (FAST ? 2 : 1) : R >= 4 ? (FAST ? 5 : 3) : 2;
 };
 
-template <int R, bool FULL, bool FAST, typename V>
-__global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<V, R, FULL, FAST>::min_blocks)
+template <int R, bool FULL, bool FAST, bool WIDE, typename V>
+__global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Threads<V, R, FULL, FAST, WIDE>::min_blocks)
     k1_part(V* __restrict__ sv, const __grid_constant__ PartProgram P) {
   using M = SmemMap<V>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -427,14 +431,16 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<
   const uint32_t sb0 = uint32_t(__cvta_generic_to_shared(smem_raw));
 
   uint64_t tile = blockIdx.x;
-  if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, deposit(tile, P.outer), s_gchunk, s_cswz, tswz, gt, per_thr);
+  // global offset of the tile being processed (computed when its copy is issued)
+  uint64_t gbase = tile < P.ntiles ? deposit(tile, P.outer) : 0;
+  if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, gbase, s_gchunk, s_cswz, tswz, gt, per_thr);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
   V v[E];
   for (; tile < P.ntiles; tile += gridDim.x) {
     const uint64_t next = tile + gridDim.x;
-    const uint64_t gbase = deposit(tile, P.outer);
+    const uint64_t gnext = next < P.ntiles ? deposit(next, P.outer) : 0;
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
       const bool last = g == P.ngroups - 1;
@@ -457,7 +463,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<
         // tile buffer per CTA leaves room for more CTAs per SM)
         __syncthreads();
         if (next < P.ntiles) {
-          issue_tile_load<V>(sv, sb0, deposit(next, P.outer), s_gchunk, s_cswz, tswz, gt, per_thr);
+          issue_tile_load<V>(sv, sb0, gnext, s_gchunk, s_cswz, tswz, gt, per_thr);
           cp_async_commit();
         }
       }
@@ -465,12 +471,12 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<
       // (uniform tests, no dispatch), then the round's other ops
       Deferred dfr;
       for (int r = G.first_round, r_end = G.first_round + G.num_rounds; r < r_end; ++r) {
-        const RoundDesc& rd = P.rounds[r];
-        const uint32_t mask = rd.mask, zmask = rd.zmask;
+        const uint64_t rw = P.rounds[r];
+        const uint32_t mask = uint32_t(rw) & 15u, zmask = (uint32_t(rw) >> 4) & 15u;
 #define SLOT(J)                                                             \
   if constexpr ((J) < R) {                                                  \
     if (mask & (1u << (J))) {                                               \
-      const double2* c = s_coef + rd.cidx[J];                               \
+      const double2* c = s_coef + (uint32_t(rw >> (24 + 10 * (J))) & 1023u); \
       if (zmask & (1u << (J)))                                              \
         rot<R, (J), true>(v, c[0], c[1]);                                   \
       else                                                                  \
@@ -479,9 +485,9 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<
   }
         SLOT(0) SLOT(1) SLOT(2) SLOT(3)
 #undef SLOT
-        for (int k = rd.first_other, k_end = rd.first_other + rd.num_other; k < k_end; ++k) {
-          const DevOp& op = P.ops[P.others[k]];
-          run_op<R, FULL, FAST>(v, op, s_coef + op.coef, thr, gbase, dfr, P);
+        const int k0 = int(rw >> 16) & 255, k1 = k0 + (int(rw >> 8) & 255);
+        for (int k = k0; k < k1; ++k) {
+          run_op<R, FULL, FAST>(v, P.ops[P.others[k]], s_coef, thr, gbase, dfr, P);
         }
       }
       apply_deferred<R>(v, dfr);
@@ -506,13 +512,14 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST>::value, K1Threads<
       }
       __syncthreads();
     }
+    gbase = gnext;
   }
   cp_async_wait<0>();
 }
 
-template <int R, bool FULL, bool FAST, typename V>
+template <int R, bool FULL, bool FAST, bool WIDE, typename V>
 int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
-  HS_TRY(smem_optin(reinterpret_cast<const void*>(k1_part<R, FULL, FAST, V>)));
+  HS_TRY(smem_optin(reinterpret_cast<const void*>(k1_part<R, FULL, FAST, WIDE, V>)));
   const int threads = 1 << (P.m - R);
   const int per_thr = ((1 << P.m) * int(sizeof(V)) / 16) / threads;
   const size_t smem = (sizeof(V) << P.m) + sizeof(double2) * P.ncoef +
@@ -520,11 +527,11 @@ int launch_k1(V* sv, const PartProgram& P, cudaStream_t s) {
                       sizeof(uint32_t) * (2 * kThrCache * threads + per_thr);
   if (smem > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K1 tile of 2^%d needs %zu B", P.m, smem);
   int per_sm = 0;
-  HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, FAST, V>, threads, smem));
+  HS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k1_part<R, FULL, FAST, WIDE, V>, threads, smem));
   if (per_sm < 1) return set_error(HS_E_UNSUPPORTED, "K1 tile does not fit an SM (m=%d)", P.m);
   const uint64_t want = uint64_t(device_sms()) * uint64_t(per_sm);
   const int grid = int(P.ntiles < want ? P.ntiles : want);
-  k1_part<R, FULL, FAST, V><<<grid, threads, smem, s>>>(sv, P);
+  k1_part<R, FULL, FAST, WIDE, V><<<grid, threads, smem, s>>>(sv, P);
   HS_CUDA(cudaGetLastError());
   return HS_OK;
 }
@@ -540,33 +547,41 @@ bool fast_program(const PartProgram& P) {
   return true;
 }
 
-template <typename V>
-int launch_typed(V* a, const PartProgram& P, cudaStream_t s) {
+template <bool WIDE, typename V>
+int launch_shape(V* a, const PartProgram& P, cudaStream_t s) {
   bool full = false;
   for (int i = 0; i < P.nops; ++i) full |= P.ops[i].kind == OP2_DENSE || P.ops[i].kind == OP2_SWAP;
   const int R = P.rbits;
   if (fast_program(P)) {
     switch (R) {
-      case 1: return launch_k1<1, false, true>(a, P, s);
-      case 2: return launch_k1<2, false, true>(a, P, s);
-      case 3: return launch_k1<3, false, true>(a, P, s);
-      default: return launch_k1<4, false, true>(a, P, s);
+      case 1: return launch_k1<1, false, true, WIDE>(a, P, s);
+      case 2: return launch_k1<2, false, true, WIDE>(a, P, s);
+      case 3: return launch_k1<3, false, true, WIDE>(a, P, s);
+      default: return launch_k1<4, false, true, WIDE>(a, P, s);
     }
   }
   if (full) {
     switch (R) {
-      case 1: return launch_k1<1, true, false>(a, P, s);
-      case 2: return launch_k1<2, true, false>(a, P, s);
-      case 3: return launch_k1<3, true, false>(a, P, s);
-      default: return launch_k1<4, true, false>(a, P, s);
+      case 1: return launch_k1<1, true, false, WIDE>(a, P, s);
+      case 2: return launch_k1<2, true, false, WIDE>(a, P, s);
+      case 3: return launch_k1<3, true, false, WIDE>(a, P, s);
+      default: return launch_k1<4, true, false, WIDE>(a, P, s);
     }
   }
   switch (R) {
-    case 1: return launch_k1<1, false, false>(a, P, s);
-    case 2: return launch_k1<2, false, false>(a, P, s);
-    case 3: return launch_k1<3, false, false>(a, P, s);
-    default: return launch_k1<4, false, false>(a, P, s);
+    case 1: return launch_k1<1, false, false, WIDE>(a, P, s);
+    case 2: return launch_k1<2, false, false, WIDE>(a, P, s);
+    case 3: return launch_k1<3, false, false, WIDE>(a, P, s);
+    default: return launch_k1<4, false, false, WIDE>(a, P, s);
   }
+}
+
+// complex128 programs whose CTAs exceed 128 threads (2^12 tiles at 16
+// amplitudes per thread) run the WIDE instantiation; complex64 has one shape
+template <typename V>
+int launch_typed(V* a, const PartProgram& P, cudaStream_t s) {
+  if (sizeof(V) == 16 && (P.m - P.rbits) > 7) return launch_shape<true>(a, P, s);
+  return launch_shape<false>(a, P, s);
 }
 
 int launch_part(void* amp, int dtype, const PartProgram& P, cudaStream_t s) {

@@ -488,20 +488,20 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
     return true;
   };
   while (left > 0) {
-    RoundDesc* rd = &P->rounds[P->nrounds++];
-    std::memset(rd, 0, sizeof(*rd));
-    rd->first_other = uint16_t(P->nothers);
+    uint32_t mask = 0, zmask = 0, cidx[4] = {0, 0, 0, 0};
+    const uint32_t first_other = uint32_t(P->nothers);
+    uint32_t num_other = 0;
     for (int b = 0; b < n; ++b) {
       const DevOp& x = P->ops[o0 + b];
-      if (state[b] || x.kind != OP1_ROT || ((rd->mask >> x.ja) & 1) || !ready(b, 1)) continue;
+      if (state[b] || x.kind != OP1_ROT || ((mask >> x.ja) & 1) || !ready(b, 1)) continue;
       // an earlier unscheduled rotation on the same bit goes first
       bool first = true;
       for (int a = 0; a < b; ++a)
         if (!state[a] && P->ops[o0 + a].kind == OP1_ROT && P->ops[o0 + a].ja == x.ja) first = false;
       if (!first) continue;
-      rd->mask |= uint8_t(1u << x.ja);
-      if (x.code < kc_y) rd->zmask |= uint8_t(1u << x.ja);
-      rd->cidx[x.ja] = x.coef;
+      mask |= 1u << x.ja;
+      if (x.code < kc_y) zmask |= 1u << x.ja;
+      cidx[x.ja] = x.coef;
       state[b] = 2;
       --left;
     }
@@ -509,13 +509,14 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
       grew = false;
       for (int b = 0; b < n; ++b) {
         if (state[b] || P->ops[o0 + b].kind == OP1_ROT || !ready(b, 2)) continue;
-        P->others[P->nothers++] = uint16_t(o0 + b);
-        ++rd->num_other;
+        P->others[P->nothers++] = uint8_t(o0 + b);
+        ++num_other;
         state[b] = 2;
         --left;
         grew = true;
       }
     }
+    P->rounds[P->nrounds++] = round_pack(mask, zmask, first_other, num_other, cidx);
     for (int b = 0; b < n; ++b)
       if (state[b] == 2) state[b] = 1;
   }

@@ -245,15 +245,18 @@ void run_program(const PartProgram& P, int ab, std::vector<C>& sv) {
         for (int e = 0; e < E; ++e) v[e] = em.ld(a0 ^ ux(e));
         uint32_t dsign = 0;
         for (int r = G.first_round; r < G.first_round + G.num_rounds; ++r) {
-          const RoundDesc& rd = P.rounds[r];
+          const uint64_t rw = P.rounds[r];
+          const uint32_t mask = uint32_t(rw) & 15u, zmask = (uint32_t(rw) >> 4) & 15u;
           for (int j = 0; j < R; ++j) {
-            if (!((rd.mask >> j) & 1)) continue;
+            if (!((mask >> j) & 1)) continue;
             DevOp rop;
             std::memset(&rop, 0, sizeof(rop));
-            rop.code = uint8_t((((rd.zmask >> j) & 1) ? kc_zy : kc_y) + j);
-            run_op(v, R, P, rop, P.coef + rd.cidx[j], thr, gbase, dsign, ab);
+            rop.code = uint8_t((((zmask >> j) & 1) ? kc_zy : kc_y) + j);
+            const uint32_t ci = uint32_t(rw >> (24 + 10 * j)) & 1023u;
+            run_op(v, R, P, rop, P.coef + ci, thr, gbase, dsign, ab);
           }
-          for (int k = rd.first_other; k < rd.first_other + rd.num_other; ++k) {
+          const int k0 = int(rw >> 16) & 255, k1 = k0 + (int(rw >> 8) & 255);
+          for (int k = k0; k < k1; ++k) {
             const DevOp& op = P.ops[P.others[k]];
             run_op(v, R, P, op, P.coef + op.coef, thr, gbase, dsign, ab);
           }
