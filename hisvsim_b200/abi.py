@@ -79,6 +79,8 @@ SIGNATURES = {
     "hs_batch_set_low_keep": [_vp, _i],
     "hs_batch_tile_caps": [_vp, _vp],
     "hs_batch_state": [_vp, _i, _vp],
+    "hs_batch_set_wait_limit": [_vp, _u32],
+    "hs_batch_block_step": [_vp, _i, _i, _i],
     "hs_batch_destroy": [_vp],
     "hs_mlp_create": [_i, ctypes.c_uint64, ctypes.POINTER(_vp)],
     "hs_mlp_num_params": [_vp],
@@ -508,6 +510,14 @@ class QaoaBatch:
 
     def set_low_keep(self, low: int):
         check(lib().hs_batch_set_low_keep(self.h, low))
+
+    def set_wait_limit(self, polls: int):
+        """Polls a work item's dependency wait makes before it gives up."""
+        check(lib().hs_batch_set_wait_limit(self.h, polls))
+
+    def block_step(self, instance: int, step: int, block: bool = True):
+        """Make (or stop making) the wait of one step unreachable (failure tests)."""
+        check(lib().hs_batch_block_step(self.h, instance, step, int(block)))
 
     def tune(self):
         cap, ctas, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()

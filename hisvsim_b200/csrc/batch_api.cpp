@@ -3,6 +3,7 @@
 // autotuner that picks the tile size and the CTA count by timing.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -28,6 +29,8 @@ struct hs_batch {
   uint8_t* d_cut = nullptr;
   unsigned long long* d_head = nullptr;
   int* d_err = nullptr;
+  uint32_t* d_limit = nullptr;   // polls of a dependency wait before it gives up
+  std::vector<BatchItem> items;  // the planned work items (host copy)
   double* d_partial = nullptr;
   double* d_expect = nullptr;
   double* h_expect = nullptr;
@@ -303,6 +306,7 @@ int build_plan(hs_batch* b) {
       total += nchunks;
     }
   b->ngroups = int(items.size());
+  b->items = items;
   b->total = total;
   b->ncounters = nc;
   HS_CUDA(cudaMalloc(&b->d_inst, sizeof(BatchInstance) * inst.size()));
@@ -325,7 +329,7 @@ int build_plan(hs_batch* b) {
   int rc = launch_batch_init(b->d_inst, b->ninst, b->stream);
   if (rc == HS_OK)
     rc = launch_batch(b->d_inst, b->d_par, b->d_items, b->ngroups, b->total, b->d_counters,
-                      b->d_head, b->d_err,
+                      b->d_head, b->d_err, b->d_limit,
                       sms * std::min(b->ctas_per_sm, batch_max_ctas_per_sm(b->threads)),
                       b->threads, b->stream);
   if (rc == HS_OK)
@@ -417,10 +421,16 @@ int hs_batch_create_qaoa(int num_instances, const int32_t* num_qubits, const int
       cudaMalloc(&b->d_par, sizeof(BatchParams) * num_instances) != cudaSuccess ||
       cudaMalloc(&b->d_head, sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_limit, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&b->d_expect, sizeof(double) * num_instances) != cudaSuccess ||
       cudaMallocHost(&b->h_expect, sizeof(double) * num_instances) != cudaSuccess ||
       cudaMallocHost(&b->h_err, sizeof(int)) != cudaSuccess)
     return fail(set_error(HS_E_NOMEM, "batch buffers"));
+  {
+    const uint32_t lim = kBatchDefaultWaitLimit;
+    if (cudaMemcpy(b->d_limit, &lim, sizeof(lim), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(set_error(HS_E_CUDA, "batch wait limit"));
+  }
   if ((rc = upload_params(b)) != HS_OK) return fail(rc);
   if ((rc = build_plan(b)) != HS_OK) return fail(rc);
   *out = b;
@@ -470,6 +480,30 @@ int hs_batch_configure(hs_batch* b, int tile_cap, int ctas_per_sm) {
     if (build_plan(b) != HS_OK) return rc;
   }
   return rc;
+}
+
+int hs_batch_set_wait_limit(hs_batch* b, uint32_t polls) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  if (polls < 1) return set_error(HS_E_INVALID, "the wait limit is at least one poll");
+  HS_CUDA(cudaStreamSynchronize(b->stream));
+  HS_CUDA(cudaMemcpy(b->d_limit, &polls, sizeof(polls), cudaMemcpyHostToDevice));
+  return HS_OK;
+}
+
+int hs_batch_block_step(hs_batch* b, int instance, int step, int block) {
+  if (!b) return set_error(HS_E_INVALID, "null batch");
+  for (size_t g = 0; g < b->items.size(); ++g) {
+    const BatchItem& it = b->items[g];
+    if (it.inst != instance || it.step != step) continue;
+    if (step < 1) return set_error(HS_E_INVALID, "the first step has no dependency");
+    // the device copy of the item: its need field alone
+    const uint32_t need = block ? 0xffffffffu : it.need;
+    HS_CUDA(cudaStreamSynchronize(b->stream));
+    HS_CUDA(cudaMemcpy(reinterpret_cast<char*>(b->d_items + g) + offsetof(BatchItem, need), &need,
+                       sizeof(need), cudaMemcpyHostToDevice));
+    return HS_OK;
+  }
+  return set_error(HS_E_INVALID, "instance %d has no step %d", instance, step);
 }
 
 int hs_batch_run(hs_batch* b, double* expect_out, double* ms) {
@@ -574,7 +608,8 @@ int hs_batch_state(hs_batch* b, int instance, void* host_out) {
 int hs_batch_destroy(hs_batch* b) {
   if (!b) return HS_OK;
   free_plan(b);
-  for (void* p : {b->pool, (void*)b->d_par, (void*)b->d_head, (void*)b->d_err, (void*)b->d_expect})
+  for (void* p : {b->pool, (void*)b->d_par, (void*)b->d_head, (void*)b->d_err, (void*)b->d_expect,
+                  (void*)b->d_limit})
     if (p) cudaFree(p);
   if (b->h_expect) cudaFreeHost(b->h_expect);
   if (b->h_err) cudaFreeHost(b->h_err);

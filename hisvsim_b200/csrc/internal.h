@@ -316,9 +316,12 @@ struct BatchItem {           // one (instance, step): its tiles in chunks, one w
   uint32_t need;             // chunks of the previous step of this instance
 };
 
+// d_limit: the polls a dependency wait makes before it gives up (device memory)
 int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
                  int nitems_groups, uint64_t total_items, uint32_t* d_counters,
-                 unsigned long long* d_head, int* d_err, int grid, int threads, cudaStream_t s);
+                 unsigned long long* d_head, int* d_err, const uint32_t* d_limit, int grid,
+                 int threads, cudaStream_t s);
+constexpr uint32_t kBatchDefaultWaitLimit = 1u << 24;
 int batch_max_ctas_per_sm(int threads);  // occupancy limit of the persistent kernel
 int launch_batch_init(const BatchInstance* d_inst, int ninst, cudaStream_t s);
 int launch_batch_expect(const BatchInstance* d_inst, int ninst, int max_n, double* d_partial,

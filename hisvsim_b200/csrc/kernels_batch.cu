@@ -24,7 +24,9 @@ namespace hisv {
 namespace {
 
 // a CTA of NT threads holds tiles of up to 16 NT amplitudes (16 per thread)
-constexpr uint32_t kDepLimit = 1u << 24;  // polls (with ~0.1 us sleeps) before giving up
+// default polls (with ~0.1 us sleeps) of a dependency wait before it gives
+// up; the batch keeps its own limit in device memory (hs_batch_set_wait_limit)
+constexpr uint32_t kDepLimit = 1u << 24;
 
 __device__ __forceinline__ uint64_t bdep(uint64_t x, const Runs& r) {
   uint64_t out = 0;
@@ -97,7 +99,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
     k6_batch(const BatchInstance* __restrict__ insts, const BatchParams* __restrict__ pars,
              const BatchItem* __restrict__ groups, int ngroups, uint64_t total,
              uint32_t* __restrict__ counters, unsigned long long* __restrict__ head,
-             int* __restrict__ err) {
+             int* __restrict__ err, const uint32_t* __restrict__ wait_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kTileMax = 16 * NT;
   constexpr int kBatchThreads = NT;
@@ -105,6 +107,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
   Shared<NT>& S = *reinterpret_cast<Shared<NT>*>(smem_raw + 2 * kTileMax * sizeof(float2));
   const int t = threadIdx.x;
   const uint32_t tiles_s = uint32_t(__cvta_generic_to_shared(tiles));
+  const uint32_t limit = *wait_limit;
   for (;;) {
     if (t == 0) {
       const unsigned long long item = atomicAdd(head, 1ull);
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(cnt) : "memory");
             if (seen >= G.need) break;
             __nanosleep(100);
-          } while (++polls < kDepLimit);
+          } while (++polls < limit);
           if (seen < G.need) {
             S.abort = 1;
             atomicExch(err, 1);
@@ -423,17 +426,18 @@ int batch_max_ctas_per_sm(int threads) {
 
 int launch_batch(const BatchInstance* d_inst, const BatchParams* d_par, const BatchItem* d_items,
                  int ngroups, uint64_t total_items, uint32_t* d_counters,
-                 unsigned long long* d_head, int* d_err, int grid, int threads, cudaStream_t s) {
+                 unsigned long long* d_head, int* d_err, const uint32_t* d_limit, int grid,
+                 int threads, cudaStream_t s) {
   if (threads == 256) {
     HS_CUDA(cudaFuncSetAttribute(k6_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(batch_smem<256>())));
     k6_batch<256><<<grid, 256, batch_smem<256>(), s>>>(d_inst, d_par, d_items, ngroups,
-                                                        total_items, d_counters, d_head, d_err);
+                                                        total_items, d_counters, d_head, d_err, d_limit);
   } else {
     HS_CUDA(cudaFuncSetAttribute(k6_batch<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(batch_smem<128>())));
     k6_batch<128><<<grid, 128, batch_smem<128>(), s>>>(d_inst, d_par, d_items, ngroups,
-                                                        total_items, d_counters, d_head, d_err);
+                                                        total_items, d_counters, d_head, d_err, d_limit);
   }
   HS_CUDA(cudaGetLastError());
   return HS_OK;

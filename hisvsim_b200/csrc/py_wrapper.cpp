@@ -28,6 +28,7 @@
 #include <complex>
 #include <cstring>
 #include <iostream>
+#include <memory>
 #include <random>
 #include <sstream>
 #include <stdexcept>
@@ -264,38 +265,76 @@ void gather_and_execute_on(SV& sv, std::vector<Bound*> gates) {
                      std::chrono::steady_clock::now() - t0).count();
 }
 
+// The proc qubits of one top-level part of the MPI drivers: the qubits the
+// part's gates do not touch, after padding the touched set with the lowest
+// other qubits up to nlocal when opt_slots is set (execute.hpp:565-571,
+// 815-821).
+std::vector<int32_t> proc_qubits(int n, int nlocal, const std::vector<hs_gate>& recs) {
+  std::vector<int> needed;
+  for (auto& r : recs) {
+    for (int i = 0; i < r.num_targets; ++i) needed.push_back(r.targets[i]);
+    for (int i = 0; i < r.num_controls; ++i) needed.push_back(r.controls[i]);
+  }
+  std::sort(needed.begin(), needed.end());
+  needed.erase(std::unique(needed.begin(), needed.end()), needed.end());
+  if (int(needed.size()) > nlocal)
+    throw py::value_error("a part touches more qubits than num_local_qubits");
+  if (g_opt_slots == 1)
+    for (int q = 0; q < n && int(needed.size()) < nlocal; ++q)
+      if (std::find(needed.begin(), needed.end(), q) == needed.end()) needed.push_back(q);
+  std::vector<int32_t> proc;
+  for (int q = 0; q < n; ++q)
+    if (std::find(needed.begin(), needed.end(), q) == needed.end()) proc.push_back(q);
+  return proc;
+}
+
 // Single-device form of gather_and_execute_on_mpi (execute.hpp:542-728): the
-// state's top n - nlocal slots play the MPI rank bits; before every part but
-// the first, the qubits outside the part (padded with the lowest qubits to
-// nlocal when opt_slots is set) become those top slots through the in-HBM
+// state's top slots play the MPI rank bits; before every part but the first,
+// the part's proc qubits become those top slots through the in-HBM
 // permutation (SvSimMPI::gather_qubits, svsim-mpi.hpp:123-173); then the part
 // runs.  Returns the final StateVector.
 SV* gather_and_execute_on_mpi(int n, int nlocal, std::vector<std::vector<Bound*>> parts) {
   if (nlocal < 1 || nlocal > n) throw py::value_error("need 1 <= num_local_qubits <= n");
-  auto* sv = new SV(n, 0);
+  auto sv = std::make_unique<SV>(n, 0);
   for (size_t p = 0; p < parts.size(); ++p) {
     auto recs = records(parts[p]);
-    std::vector<int> needed;
-    for (auto& r : recs) {
-      for (int i = 0; i < r.num_targets; ++i) needed.push_back(r.targets[i]);
-      for (int i = 0; i < r.num_controls; ++i) needed.push_back(r.controls[i]);
-    }
-    std::sort(needed.begin(), needed.end());
-    needed.erase(std::unique(needed.begin(), needed.end()), needed.end());
-    if (int(needed.size()) > nlocal) {
-      delete sv;
-      throw py::value_error("a part touches more qubits than num_local_qubits");
-    }
-    for (int q = 0; q < n && int(needed.size()) < nlocal; ++q)  // execute.hpp:565-571
-      if (std::find(needed.begin(), needed.end(), q) == needed.end()) needed.push_back(q);
-    std::vector<int32_t> proc;
-    for (int q = 0; q < n; ++q)
-      if (std::find(needed.begin(), needed.end(), q) == needed.end()) proc.push_back(q);
+    const std::vector<int32_t> proc = proc_qubits(n, nlocal, recs);
     py::gil_scoped_release nogil;
-    if (p > 0 && !proc.empty()) check(hs_gather_qubits(sv->st, proc.data(), int(proc.size()), nullptr));
+    if (p > 0 && !proc.empty())
+      check(hs_gather_qubits(sv->st, proc.data(), int(proc.size()), nullptr));
     check(hs_part_run(sv->st, recs.data(), int(recs.size()), nullptr));
   }
-  return sv;
+  return sv.release();
+}
+
+// Single-device form of gather_and_execute_multilevel_on_mpi
+// (execute.hpp:730-900): multi_parts[p][0] lists every gate of top-level part
+// p and decides its proc qubits (gathered to the top slots before every top
+// part but the first); multi_parts[p][1..] are its second-level parts, run in
+// order (the reference runs each with gather_and_execute_on_multi,
+// execute.hpp:867).  Here the second-level parts of one top part go to the
+// device as one hs_parts_run call.  Returns the final StateVector.
+SV* gather_and_execute_multilevel_on_mpi(int n, int nlocal,
+                                         std::vector<std::vector<std::vector<Bound*>>> multi) {
+  if (nlocal < 1 || nlocal > n) throw py::value_error("need 1 <= num_local_qubits <= n");
+  auto sv = std::make_unique<SV>(n, 0);
+  for (size_t p = 0; p < multi.size(); ++p) {
+    if (multi[p].empty()) throw py::value_error("a top-level part needs its gate list first");
+    const std::vector<int32_t> proc = proc_qubits(n, nlocal, records(multi[p][0]));
+    std::vector<hs_gate> flat;
+    std::vector<int32_t> offs{0};
+    for (size_t i = 1; i < multi[p].size(); ++i) {
+      auto r = records(multi[p][i]);
+      flat.insert(flat.end(), r.begin(), r.end());
+      offs.push_back(int32_t(flat.size()));
+    }
+    py::gil_scoped_release nogil;
+    if (p > 0 && !proc.empty())
+      check(hs_gather_qubits(sv->st, proc.data(), int(proc.size()), nullptr));
+    if (offs.size() > 1)
+      check(hs_parts_run(sv->st, flat.data(), offs.data(), int(offs.size()) - 1, nullptr));
+  }
+  return sv.release();
 }
 
 }  // namespace
@@ -342,6 +381,8 @@ PYBIND11_MODULE(svsimulator_py_wrapper, m) {
       .def("apply", &Bound::apply);
   m.def("gather_and_execute_on", &gather_and_execute_on);
   m.def("gather_and_execute_on_mpi", &gather_and_execute_on_mpi,
+        py::return_value_policy::take_ownership);
+  m.def("gather_and_execute_multilevel_on_mpi", &gather_and_execute_multilevel_on_mpi,
         py::return_value_policy::take_ownership);
   m.def("obtain_apply_time", []() {
     long long us = 0;

@@ -319,6 +319,17 @@ int hs_batch_tile_caps(hs_batch* b, int32_t* caps);
  * instance i; *ms = device time of the run between CUDA events on the
  * batch's stream, read-back of the results included (may be NULL). */
 int hs_batch_run(hs_batch* b, double* expect_out, double* ms);
+/* Failure detection of the persistent launch.  A work item waits (bounded)
+ * until every chunk of the previous step of its instance is done; after
+ * `polls` polls (~0.1 us apart; default 2^24) it gives up, the launch ends
+ * early and hs_batch_run returns HS_E_TIMEOUT, leaving the device usable.
+ * hs_batch_set_wait_limit sets that bound. */
+int hs_batch_set_wait_limit(hs_batch* b, uint32_t polls);
+/* Test hook for the above: block = 1 makes the wait of step `step` (>= 1) of
+ * `instance` unreachable (its need count exceeds what the previous step can
+ * complete), block = 0 restores the planned count.  No counterpart in the
+ * reference. */
+int hs_batch_block_step(hs_batch* b, int instance, int step, int block);
 /* {work items, steps, bytes moved per run, tile cap, CTAs per SM, tiles per
  * item, lowest qubits kept in later passes' tiles, threads per CTA} */
 int hs_batch_stats(hs_batch* b, int64_t* stats);

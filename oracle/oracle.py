@@ -61,6 +61,8 @@ class RefOracle:
         self.lib.ref_run.restype = _c_int
         self.lib.ref_probability.argtypes = [_c_int, _p, _c_int, _c_int]
         self.lib.ref_probability.restype = ctypes.c_double
+        self.lib.ref_project.argtypes = [_c_int, _p, _p, _p, _c_int, _c_int, _p]
+        self.lib.ref_project.restype = _c_int
         self.gate_size = self.lib.ref_hs_gate_size()
 
     def run(self, n, gates, offsets=None, mode=0, opt_slots=0, threads=None,
@@ -77,6 +79,19 @@ class RefOracle:
     def probability(self, n, state, qubit, value=0):
         state = np.ascontiguousarray(state, dtype=np.complex128)
         return self.lib.ref_probability(n, _ptr(state), qubit, value)
+
+    def project(self, n, state, qubits, values, renormalize=True):
+        """StateVector::project (state_vector.hpp:829-894): the reference's
+        projected state over the remaining qubits (it divides by p)."""
+        state = np.ascontiguousarray(state, dtype=np.complex128)
+        q = np.ascontiguousarray(qubits, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.int32)
+        out = np.zeros(1 << (n - len(q)), dtype=np.complex128)
+        rc = self.lib.ref_project(n, _ptr(state), _ptr(q), _ptr(v), len(q), int(renormalize),
+                                  _ptr(out))
+        if rc != 0:
+            raise ValueError("reference rejected the projection")
+        return out
 
 
 class PortOracle:

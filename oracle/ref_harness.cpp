@@ -170,4 +170,27 @@ double ref_probability(int n, const double* state, int qubit, int value) {
   return p;
 }
 
+// StateVector::project(qubits, values, renormalize) of the reference
+// (state_vector.hpp:829-894) on a given state: out receives the projected
+// state over the remaining 2^(n-k) indices, in the order of the reference's
+// own loop over the remaining qubits (qubit_loop, trip_count).
+int ref_project(int n, const double* state, const int32_t* qubits, const int32_t* values, int k,
+                int renormalize, double* out) {
+  if (n < 2 || k < 1 || k >= n) return -1;
+  QuietCout quiet;
+  set_num_threads(1);
+  set_init_num_threads(1);
+  StateVector sv(n, 0);
+  Type* before = sv.state();
+  std::memcpy(before, state, (size_t(1) << n) * sizeof(Type));
+  std::vector<Qubit> q(qubits, qubits + k);
+  std::vector<int> v(values, values + k);
+  sv.project(q, v, renormalize != 0);
+  Type* after = sv.state();
+  std::memcpy(out, after, (size_t(1) << (n - k)) * sizeof(Type));
+  free(after);
+  free(before);
+  return 0;
+}
+
 }  // extern "C"

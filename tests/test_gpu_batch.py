@@ -110,3 +110,72 @@ def test_tuner_and_mixed_sizes():
     assert st["items"] > 0 and st["bytes_per_run"] > 0
     check_batch(b, insts, states=False)
     b.close()
+
+
+def hc_from_amplitudes(n, amps, edges):
+    """<H_C> = sum_E (1 - <Z_a Z_b>)/2 from qubit-ordered amplitudes (FP64)."""
+    p = np.abs(np.asarray(amps, dtype=np.complex128)) ** 2
+    idx = np.arange(1 << n, dtype=np.int64)
+    total = 0.0
+    for a, b in edges:
+        parity = ((idx >> a) ^ (idx >> b)) & 1
+        zz = float(np.sum(p * (1 - 2 * parity)))
+        total += (1.0 - zz) / 2.0
+    return total
+
+
+def test_batch_against_reference_oracle(ref):
+    """K6 pinned to the reference itself: the same QAOA gate list (H on every
+    qubit, then per round RZZ(gamma) on each edge and RX(2 beta) on each qubit,
+    basic_gates.hpp:341-363,1235-1313) run through the reference's own
+    BoundGate::apply (RefOracle), for instances of <= 16 qubits; amplitudes to
+    1e-5 and <H_C> to 1e-5 per edge, with no plain-form run in between."""
+    from hisvsim_b200.gates import to_records
+
+    insts = make_instances([8, 11, 12, 15, 16, 13], 4, 9100)
+    b = abi.QaoaBatch([(n, e, g, bt) for n, e, g, bt, _ in insts], 4)
+    hc, _ = b.run()
+    for i, (n, edges, _, _, gates) in enumerate(insts):
+        want = ref.run(n, to_records(gates), mode=0)
+        got = b.state(i)
+        assert np.abs(got - want).max() <= AMP_TOL, (i, n)
+        hw = hc_from_amplitudes(n, want, edges)
+        assert abs(hc[i] - hw) <= HC_TOL * len(edges), (i, n, hc[i], hw)
+    b.close()
+
+
+def test_dependency_wait_timeout_is_reported_and_recovers():
+    """Failure detection without a GPU fault: one step's dependency wait is
+    made unreachable from the host and the poll limit shortened, so the
+    persistent launch gives up, ends and reports HS_E_TIMEOUT; with the step
+    restored, the next run of the same captured graph returns the same
+    <H_C> as before."""
+    insts = make_instances([10, 12, 14, 16], 3, 777)
+    b = abi.QaoaBatch([(n, e, g, bt) for n, e, g, bt, _ in insts], 3)
+    b.configure(10, 4)
+    good, _ = b.run()
+    b.set_wait_limit(2000)  # ~0.2 ms of polls
+    b.block_step(2, 1)
+    with pytest.raises(abi.HisvError) as e:
+        b.run()
+    assert e.value.code == abi.HS_E_TIMEOUT
+    b.block_step(2, 1, block=False)
+    b.set_wait_limit(1 << 24)
+    again, _ = b.run()
+    assert np.array_equal(good, again)
+    for i, (n, edges, _, _, gates) in enumerate(insts):
+        want = hc_c128(plain_c128(n, gates), edges)
+        assert abs(again[i] - want) <= HC_TOL * len(edges)
+    b.close()
+
+
+def test_wait_hooks_reject_bad_arguments():
+    insts = make_instances([8, 9], 2, 5)
+    b = abi.QaoaBatch([(n, e, g, bt) for n, e, g, bt, _ in insts], 2)
+    with pytest.raises(abi.HisvError):
+        b.set_wait_limit(0)
+    with pytest.raises(abi.HisvError):
+        b.block_step(0, 0)  # the first step waits for nothing
+    with pytest.raises(abi.HisvError):
+        b.block_step(5, 1)  # no such instance
+    b.close()

@@ -83,3 +83,30 @@ def test_mpi_driver_emulation(svsim, port):
     sim = svsim.gather_and_execute_on_mpi(n, nlocal, lists)
     want = port.run(n, to_records(gates))
     assert np.abs(sim.amplitudes() - want).max() <= 1e-12
+
+
+@pytest.mark.parametrize("opt_slots", [0, 1])
+def test_multilevel_mpi_driver_matches_reference(svsim, ref, opt_slots):
+    """gather_and_execute_multilevel_on_mpi (py_wrapper.cpp:158-161,
+    execute.hpp:730-900) on one device: top-level parts of <= 8 qubits, each
+    split into second-level parts of <= 4 qubits; every top part after the
+    first gathers its proc qubits to the top slots (K2), its second-level
+    parts run through K1.  Compared with the reference's own per-gate path."""
+    n, nlocal = 13, 9
+    gates = circuits.random_layered(n, 6, 29)
+    top = partition.partition_acyclic(gates, 8)
+    multi = []
+    for p in top:
+        sub_gates = [gates[i] for i in p]
+        second = partition.partition_acyclic(sub_gates, 4)
+        multi.append([[bound(svsim, g) for g in sub_gates]] +
+                     [[bound(svsim, sub_gates[i]) for i in s] for s in second])
+    svsim.set_opt_slots(opt_slots)
+    try:
+        sim = svsim.gather_and_execute_multilevel_on_mpi(n, nlocal, multi)
+    finally:
+        svsim.set_opt_slots(0)
+    want = ref.run(n, to_records(gates), mode=0)
+    assert np.abs(sim.amplitudes() - want).max() <= 1e-12
+    with pytest.raises(ValueError):
+        svsim.gather_and_execute_multilevel_on_mpi(n, 3, multi)  # parts wider than nlocal

@@ -166,3 +166,26 @@ def test_project_rejects_bad_arguments():
     for q, v in ([[0, 0], [0, 1]], [[5], [0]], [[1], [2]], [[0, 1, 2, 3], None]):
         with pytest.raises(abi.HisvError):
             st.project(q, v)
+
+
+@pytest.mark.parametrize("renormalize", [True, False])
+@pytest.mark.parametrize("permuted", [False, True])
+def test_project_matches_reference_project(ref, renormalize, permuted):
+    """hs_project with the reference's normalisation (mode 1: divide by p;
+    mode 2: renormalize=false) against StateVector::project itself
+    (state_vector.hpp:829-894, through the oracle harness) on the same state,
+    at 1e-12; the device state's slots are permuted in one case."""
+    from hisvsim_b200.gates import to_records
+
+    n = 10
+    gates = circuits.random_layered(n, 5, 41)
+    full = ref.run(n, to_records(gates))
+    st = abi.State(n, abi.C128)
+    st.load(full)
+    if permuted:
+        st.permute_bits([(1, 8), (3, 6)])
+    for qubits, values in (([4], [1]), ([7, 0, 2], [0, 1, 1]), ([9, 5], [1, 1])):
+        sub, p = st.project(qubits, values, 1 if renormalize else 2)
+        want = ref.project(n, full, qubits, values, renormalize)
+        assert np.abs(sub.amplitudes() - want).max() <= 1e-12
+        sub.close()

@@ -80,6 +80,7 @@ def test_pymod_surface():
     for name in ["AggregateGate_0", "AggregateGate_1", "AggregateGate_2", "AggregateGate_3",
                  "AggregateGate_C1", "AggregateGate_C2", "AggregateGate_Frac",
                  "AggregateGateFactory", "StateVector", "BoundGate", "gather_and_execute_on",
+                 "gather_and_execute_on_mpi", "gather_and_execute_multilevel_on_mpi",
                  "obtain_apply_time", "obtain_gate_counter", "obtain_move_counter",
                  "obtain_gather_time", "set_num_threads", "set_init_num_threads",
                  "set_opt_slots"]:
