@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-qubits", type=int, default=26, help="size of the CPU sample")
     ap.add_argument("--cpu-layers", type=int, default=8)
+    ap.add_argument("--cpu-full-qubits", type=int, default=30,
+                    help="state size of the full-size CPU rate (16 GiB at 30)")
+    ap.add_argument("--cpu-full-layers", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--tile-qubits", type=int, default=0, help="K1 tile bits (0 = automatic)")
@@ -173,26 +176,47 @@ def workload(n, layers, seed, k, split=None):
     return gates, parts, rec, offs
 
 
-def cpu_sample(args, threads):
-    """The reference's own CPU path (oracle/_ref, BoundGate::apply per gate and
-    gather_and_execute_on_multi per part) on a bounded sample of the workload."""
+def cpu_sample(args, threads, full_size=False):
+    """The reference's own CPU path (oracle/_ref: its headers compiled here) on
+    a bounded sample of the workload, through both of its live entry points on
+    the same circuit and parts the GPU runs: per-gate BoundGate::apply
+    (state_vector.hpp:1349) and the part path gather_and_execute_on_multi
+    (execute.hpp:318-470) with opt_slots=1.  With full_size, also the
+    per-gate path on a --cpu-full-qubits state (a few layers)."""
     from oracle.oracle import RefOracle
 
-    n, layers = args.cpu_qubits, args.cpu_layers
-    gates, parts, rec, offs = workload(n, layers, args.seed, min(args.part_qubits, n))
     from hisvsim_b200.gates import to_records
 
+    n, layers = args.cpu_qubits, args.cpu_layers
+    gates, parts, rec, offs = workload(n, layers, args.seed, min(args.part_qubits, n),
+                                       partitioner(args))
     ref = RefOracle()
-    flat = to_records(gates)
-    t = time.perf_counter()
-    ref.run(n, flat, mode=0, threads=threads)
-    t_gate = time.perf_counter() - t
     upd = len(gates) * float(1 << n)
-    return {"value": upd / t_gate, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"{n} qubits x {layers} layers of the same circuit family "
-                      f"({len(gates)} gates), per-gate BoundGate::apply "
-                      f"(state_vector.hpp:1349), {t_gate:.2f} s",
-            "seconds": t_gate}
+    t = time.perf_counter()
+    ref.run(n, to_records(gates), mode=0, threads=threads)
+    t_gate = time.perf_counter() - t
+    t = time.perf_counter()
+    ref.run(n, rec, offs, mode=1, opt_slots=1, threads=threads)
+    t_part = time.perf_counter() - t
+    out = {"value": upd / t_gate, "unit": UNIT, "cores": threads, "kind": "reference",
+           "sample": f"{n} qubits x {layers} layers of the same circuit family ({len(gates)} gates, "
+                     f"{len(parts)} parts of <= {args.part_qubits} qubits), all host threads",
+           "seconds": t_gate,
+           "per_gate": {"entry": "BoundGate::apply (state_vector.hpp:1349)", "seconds": t_gate,
+                        "value": upd / t_gate},
+           "parts": {"entry": "gather_and_execute_on_multi, opt_slots=1 (execute.hpp:318-470)",
+                     "seconds": t_part, "value": upd / t_part, "parts": len(parts)}}
+    if full_size:
+        nf, lf = args.cpu_full_qubits, args.cpu_full_layers
+        fg = workload(nf, lf, args.seed, min(args.part_qubits, nf), partitioner(args))[0]
+        t = time.perf_counter()
+        ref.run(nf, to_records(fg), mode=0, threads=threads)
+        t_full = time.perf_counter() - t
+        out["full_size"] = {"entry": "BoundGate::apply", "qubits": nf, "layers": lf,
+                            "gates": len(fg), "seconds": t_full,
+                            "value": len(fg) * float(1 << nf) / t_full,
+                            "state_bytes": (1 << nf) * 16}
+    return out
 
 
 def run_reference_arm(args):
@@ -200,11 +224,13 @@ def run_reference_arm(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     threads = os.cpu_count() or 1
-    vals = []
+    vals, parts_vals = [], []
+    r = None
     for i in range(args.warmup + args.steps):
         r = cpu_sample(args, threads)
         if i >= args.warmup:
             vals.append(r["value"])
+            parts_vals.append(r["parts"]["value"])
     v = statistics.mean(vals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -215,7 +241,10 @@ def run_reference_arm(args):
                                    f"and ~2 h of CPU per step)",
                        "parallelism": "replicas"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": r["sample"]},
+                             "sample": r["sample"] + "; value = per-gate BoundGate::apply, "
+                                       "the faster of the reference's two live paths"},
+            "parts_path": {"entry": r["parts"]["entry"], "value": statistics.mean(parts_vals),
+                           "unit": UNIT},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -355,9 +384,19 @@ def learned_form(args, abi, pg, device):
         for k in ks:
             res[k] = learned.measure(st, gates, partition.partition_acyclic(gates, k), reps=1,
                                      warmup=0)
+        # the method without the network: the same DP with a trivial cost
+        # (fewest parts), and DFS-order parts at every size (best measured)
+        fewest = learned.propose_fewest(gates, n)
+        t_fewest = learned.measure(st, gates, fewest["parts"], reps=1, warmup=0)
+        t_dfs = {k: learned.measure(st, gates, partition.partition_dfs(gates, k), reps=1, warmup=0)
+                 for k in (8, 9, 10, 11, 12)}
     st.close()
     model.close()
     best_k = min(res, key=res.get)
+    best_dfs = min(t_dfs, key=t_dfs.get)
+    nonlearned = {"dp_fewest_parts_s": t_fewest, "dfs_s": {str(k): v for k, v in t_dfs.items()},
+                  "best_dfs_k": best_dfs, f"acyclic_best_k{best_k}_s": res[best_k]}
+    best_nonlearned = min(t_fewest, t_dfs[best_dfs], res[best_k])
     return {"harvest_parts": int(len(y)), "harvest_qubits": "24..32", "harvest_s": t_h,
             "train_s": t_t, "final_train_mse": float(losses[-1]), "holdout_mean_rel_err": rel,
             "eval": f"random U3+CZ circuit {n} qubits x 40 layers, complex64",
@@ -366,6 +405,8 @@ def learned_form(args, abi, pg, device):
             "acyclic_s": {str(k): v for k, v in res.items()},
             "gain_vs_acyclic_k9": res[9] / t_learned,
             "gain_vs_best_acyclic": res[best_k] / t_learned, "best_acyclic_k": best_k,
+            "nonlearned": nonlearned,
+            "gain_vs_best_nonlearned": best_nonlearned / t_learned,
             "clocks": clk.summary()}
 
 
@@ -572,7 +613,8 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_sample(args, os.cpu_count() or 1)
+            cpu = cpu_sample(args, os.cpu_count() or 1,
+                             full_size=host_available_bytes() > (1 << args.cpu_full_qubits) * 16 * 1.5)
         except Exception as ex:  # the oracle library may be missing
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {ex}"}

@@ -991,6 +991,329 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
   if (warp == 0) tc::tmem_dealloc(tmem, 2 * kK4DirectCols);
 }
 
+// ---- K4, two unitaries per pass, bulk-loaded --------------------------------------
+// The bulk-loaded pipeline applied twice to each tile before it leaves the
+// SM: the first product's accumulator goes back into the tile's shared
+// buffer as complex64 (in tile-index order, like the loaded tile), is split
+// again into the BF16 operand of the second unitary (whose six bits are
+// other tile bits) and only the second product is stored to HBM.  Tiles of
+// 2^12 amplitudes; both 128 x 128 real-form operands A1, A2 stay in shared
+// memory; two ring buffers; four TMEM accumulators (stage x tile parity).
+// Each role runs its steps in a skewed order, every step waiting only on
+// earlier steps of the other roles:
+//   loader      L(i)  waits bfree(i-2)  (the second MMA of tile i-2 read its buffer)
+//   producers   P1(i) waits rfull(i);   P2(i-1) waits rmid(i-1)
+//   MMA         M1(i) waits bfull1(i), tfree1(i-2);  M2(i-1) waits bfull2(i-1), tfree2(i-3)
+//   epilogue    MID(i) waits mdone1(i) and writes the buffer (rmid);
+//               FIN(i-1) waits mdone2(i-1) and stores to HBM
+// Every wait is bounded; a timeout sets the error flag and the abort word.
+constexpr int kBulk2Threads = 576;     // 8 producer, 8 epilogue, 1 MMA, 1 loader warps
+constexpr int kBulk2MaxTileBits = 12;  // N <= 64 columns
+constexpr int kBulk2Items = 4;         // B items per producer thread (N * 16 / 256)
+
+__global__ void __launch_bounds__(kBulk2Threads, 1)
+    k4_bulk2(float2* __restrict__ sv, const __grid_constant__ FusedPass P,
+             const uint8_t* __restrict__ a_all, int* __restrict__ err, int chunk_bits) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m = P.m, T = 1 << m;
+  const int N = 1 << (m - kFusedBits);
+  const int lgN = m - kFusedBits;
+  const uint32_t bk = uint32_t(N) * 16u;
+  const uint32_t bbytes = uint32_t(N) * 256u;
+  const int nchunks = T >> chunk_bits;
+  const uint32_t chunk_bytes = 8u << chunk_bits;
+  uint8_t* sA = sm;                       // [2][kFusedABytes]
+  uint8_t* sB = sA + 2 * kFusedABytes;    // [2][T * 8]: raw tile / B operand
+  uint64_t* gc = reinterpret_cast<uint64_t*>(sB + size_t(T) * 16);  // global offset of chunk c
+  uint64_t* gp2 = gc + nchunks;           // global offset of stage-2 part index p
+  uint64_t* gn2 = gp2 + 64;               // global offset of stage-2 column n
+  uint32_t* tq = reinterpret_cast<uint32_t*>(gn2 + N);  // [2][64]: tile index of part index p
+  uint32_t* tn = tq + 128;                // [2][N]: tile index of column n
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tn + 2 * N + (N & 1));
+  uint64_t* rfull = bars;        // [2] loader -> producers
+  uint64_t* bfull1 = bars + 2;   // [2] producers (stage 1) -> MMA
+  uint64_t* rmid = bars + 4;     // [2] epilogue (stage 1 result in the buffer) -> producers
+  uint64_t* bfull2 = bars + 6;   // [2] producers (stage 2) -> MMA
+  uint64_t* bfree = bars + 8;    // [2] MMA (stage 2 read the buffer) -> loader
+  uint64_t* mdone = bars + 10;   // [2 stages][2] MMA -> epilogue
+  uint64_t* tfree = bars + 14;   // [2 stages][2] epilogue -> MMA
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 18);
+  uint32_t* tmem_base = reinterpret_cast<uint32_t*>(bars + 19);
+  float* stage = reinterpret_cast<float*>(bars + 20);  // [8 warps][kBulkStageFloats]
+
+  for (int s2 = 0; s2 < 2; ++s2) {
+    const uint4* src = reinterpret_cast<const uint4*>(a_all + size_t(P.part[s2]) * kFusedABytes);
+    uint4* dst = reinterpret_cast<uint4*>(sA + size_t(s2) * kFusedABytes);
+    for (int i = t; i < kFusedABytes / 16; i += kBulk2Threads) dst[i] = src[i];
+  }
+  for (int s2 = 0; s2 < 2; ++s2) {
+    uint32_t pmask = 0;
+    for (int b = 0; b < kFusedBits; ++b) pmask |= 1u << P.pbits[s2][b];
+    for (int p = t; p < 64; p += kBulk2Threads) {
+      uint32_t x = 0;
+      for (int b = 0; b < kFusedBits; ++b) x |= uint32_t((p >> b) & 1) << P.pbits[s2][b];
+      tq[s2 * 64 + p] = x;
+      if (s2 == 1) gp2[p] = dep(x, P.tile);
+    }
+    for (int nn = t; nn < N; nn += kBulk2Threads) {
+      uint32_t x = 0;
+      int bit = 0;
+      for (int b = 0; b < m; ++b)
+        if (!((pmask >> b) & 1)) x |= uint32_t((nn >> bit++) & 1) << b;
+      tn[s2 * N + nn] = x;
+      if (s2 == 1) gn2[nn] = dep(x, P.tile);
+    }
+  }
+  for (int c = t; c < nchunks; c += kBulk2Threads) gc[c] = dep(uint64_t(c) << chunk_bits, P.tile);
+  if (t == 0) {
+    for (int b = 0; b < 2; ++b) {
+      // short runs: one cp.async arrival per loader lane; long runs: one
+      // arrival with the tile's byte count
+      tc::mbar_init(&rfull[b], (8u << chunk_bits) < 1024u ? 32 : 1);
+      tc::mbar_init(&bfull1[b], kWsProducers);
+      tc::mbar_init(&rmid[b], kWsProducers);  // the epilogue has as many threads
+      tc::mbar_init(&bfull2[b], kWsProducers);
+      tc::mbar_init(&bfree[b], 1);
+    }
+    for (int b = 0; b < 4; ++b) {
+      tc::mbar_init(&mdone[b], 1);
+      tc::mbar_init(&tfree[b], kWsProducers);
+    }
+    *abort_flag = 0;
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tmem_base, 4 * 64);
+    tc::tmem_relinquish();
+  }
+  tc::fence_proxy_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_base;
+  // accumulator of stage s (0, 1) for tile parity b
+  auto acc = [&](int s, int b) { return tmem + uint32_t(2 * s + b) * 64u; };
+  const uint64_t cnt =
+      blockIdx.x < P.ntiles ? (P.ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  auto tile_of = [&](uint64_t i) { return blockIdx.x + i * gridDim.x; };
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicExch(err, 1);
+  };
+  auto ph = [](uint64_t i) { return uint32_t(i >> 1) & 1u; };  // phase parity of tile i's barriers
+
+  if (warp == 17) {
+    // ---- loader: runs of 1 KiB or more as bulk copies (complete_tx on
+    // rfull); shorter runs as 16-byte cp.async copies, each lane's completing
+    // on rfull through cp.async.mbarrier.arrive (rfull then counts the lanes)
+    const bool small = chunk_bytes < 1024u;
+    uint64_t issued = 0;
+    for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
+      const int b = int(i & 1);
+      if (i >= 2 && !tc::mbar_wait(&bfree[b], ph(i - 2), kWaitLimit)) {
+        fail();
+        break;
+      }
+      const float2* base = sv + dep(tile_of(i), P.outer);
+      const uint32_t dst = tc::smem_u32(sB + size_t(b) * T * 8);
+      if (small) {
+        const int per_chunk = int(chunk_bytes >> 4);  // 16-byte pieces per run
+        for (int u = lane; u < (T >> 1); u += 32) {
+          const int c = u / per_chunk, w = u - c * per_chunk;
+          cp_async16(dst + uint32_t(u) * 16u, base + gc[c] + 2 * w);
+        }
+        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
+                         tc::smem_u32(&rfull[b]))
+                     : "memory");
+      } else {
+        if (lane == 0) tc::mbar_arrive_expect_tx(&rfull[b], uint32_t(T) * 8u);
+        __syncwarp();
+        for (int c = lane; c < nchunks; c += 32)
+          tc::bulk_load(dst + uint32_t(c) * chunk_bytes, base + gc[c], chunk_bytes, &rfull[b]);
+      }
+      issued = i + 1;
+    }
+    for (uint64_t j = issued > 2 ? issued - 2 : 0; j < issued; ++j)
+      tc::mbar_wait(&rfull[j & 1], ph(j), kWaitLimit);
+    if (small) cp_async_wait0();
+  } else if (warp < 8) {
+    // ---- producers: stage s of tile i reads the raw tile (s = 0: as loaded,
+    // s = 1: the first product) and writes stage s's BF16 hi / lo operand
+    const int nitems = (N * 16) / kWsProducers;  // 1..4
+    auto produce = [&](int s2, uint64_t i) -> bool {
+      const int b = int(i & 1);
+      uint64_t* wait_bar = s2 == 0 ? &rfull[b] : &rmid[b];
+      const bool ok = !*abort_flag && tc::mbar_wait(wait_bar, ph(i), kWaitLimit);
+      if (!ok) fail();
+      uint8_t* buf = sB + size_t(b) * T * 8;
+      const uint32_t* tqs = tq + s2 * 64;
+      const uint32_t* tns = tn + s2 * N;
+      float2 x[kBulk2Items][4];
+#pragma unroll
+      for (int k = 0; k < kBulk2Items; ++k) {
+        if (k >= nitems) break;
+        const int item = t + k * kWsProducers;
+        const int kb = item >> lgN, nn = item & (N - 1);
+        const uint32_t tcol = tns[nn];
+        const uint4 tp = *reinterpret_cast<const uint4*>(tqs + 4 * kb);
+        x[k][0] = *reinterpret_cast<const float2*>(buf + size_t(tp.x | tcol) * 8);
+        x[k][1] = *reinterpret_cast<const float2*>(buf + size_t(tp.y | tcol) * 8);
+        x[k][2] = *reinterpret_cast<const float2*>(buf + size_t(tp.z | tcol) * 8);
+        x[k][3] = *reinterpret_cast<const float2*>(buf + size_t(tp.w | tcol) * 8);
+      }
+      uint32_t stop;
+      asm volatile(
+          "{\n .reg .pred p, q;\n setp.eq.u32 p, %1, 0;\n"
+          " bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+          : "=r"(stop)
+          : "r"(uint32_t(ok)), "n"(kWsProducers)
+          : "memory");
+      if (stop) return false;
+      uint8_t* bl = buf + bbytes;
+#pragma unroll
+      for (int k = 0; k < kBulk2Items; ++k) {
+        if (k >= nitems) break;
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x[k][q].x, x[k][q].y);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(x[k][q].x - hf.x, x[k][q].y - hf.y);
+          hw[q] = *reinterpret_cast<const uint32_t*>(&h);
+          lw[q] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+        const int item = t + k * kWsProducers;
+        const uint32_t boff = tc::kmajor_off(uint32_t(item & (N - 1)), uint32_t((item >> lgN) * 8), bk);
+        *reinterpret_cast<uint4*>(buf + boff) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(bl + boff) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+      }
+      tc::fence_proxy_async_smem();
+      mbar_arrive(s2 == 0 ? &bfull1[b] : &bfull2[b]);
+      return true;
+    };
+    bool go = true;
+    for (uint64_t i = 0; i < cnt && go; ++i) {
+      go = produce(0, i);
+      if (go && i >= 1) go = produce(1, i - 1);
+    }
+    if (go && cnt > 0) produce(1, cnt - 1);
+  } else if (warp < 16) {
+    // ---- epilogue: stage 0's accumulator back into the tile buffer (in tile
+    // index order), stage 1's to HBM; both through the per-warp staging
+    // transpose of k4_bulk (two memory-adjacent amplitudes per lane)
+    const int quad = warp & 3, half = (warp - 8) >> 2;
+    const int comp = lane & 1, pl = lane >> 1;
+    const int per = N / 2 < 16 ? 16 : N / 2;
+    const int c_begin = half * per;
+    const int c_end = c_begin + per < N ? c_begin + per : N;
+    float* stg = stage + (warp - 8) * kBulkStageFloats;
+    auto sidx = [](int p, int c) { return p * 32 + ((c ^ ((p & 7) << 1)) << 1); };
+    auto drain = [&](int s2, uint64_t i) -> bool {
+      const int b = int(i & 1);
+      if (!tc::mbar_wait(&mdone[2 * s2 + b], ph(i), kWaitLimit)) {
+        fail();
+        return false;
+      }
+      tc::tc_fence_after();
+      // destination of amplitude (p, c): global offset (stage 1) or the tile
+      // index in the buffer (stage 0)
+      const bool to_smem = s2 == 0;
+      const uint32_t* tqs = tq + quad * 16;            // stage 0 rows
+      const uint32_t* tns = tn;                        // stage 0 columns
+      const uint64_t* gpq = gp2 + quad * 16;           // stage 1 rows
+      const bool pairs = to_smem ? (tn[1] == 1) : (gn2[1] == 1);
+      float2* tb = sv + dep(tile_of(i), P.outer);
+      float2* sbuf = reinterpret_cast<float2*>(sB + size_t(b) * T * 8);
+      for (int c0 = c_begin; c0 + 16 <= c_end; c0 += 16) {
+        float d[16];
+        tc::tmem_ld16(acc(s2, b) + (uint32_t(quad * 32) << 16) + uint32_t(c0), d);
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 16; ++c) stg[sidx(pl, c) + comp] = d[c];
+        __syncwarp();
+#pragma unroll
+        for (int s4 = 0; s4 < 4; ++s4) {
+          int p, c;
+          float4 v;
+          if (pairs) {
+            p = (lane >> 3) + 4 * s4;
+            c = 2 * (lane & 7);
+            v = *reinterpret_cast<const float4*>(stg + sidx(p, c));
+          } else {
+            p = 2 * ((lane >> 4) + 2 * s4);
+            c = lane & 15;
+            const float2 lo = *reinterpret_cast<const float2*>(stg + sidx(p, c));
+            const float2 hi = *reinterpret_cast<const float2*>(stg + sidx(p + 1, c));
+            v = make_float4(lo.x, lo.y, hi.x, hi.y);
+          }
+          if (to_smem)
+            *reinterpret_cast<float4*>(sbuf + (tqs[p] | tns[c0 + c])) = v;
+          else
+            __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn2[c0 + c]), v);
+        }
+      }
+      tc::tc_fence_before();
+      mbar_arrive(&tfree[2 * s2 + b]);
+      if (to_smem) mbar_arrive(&rmid[b]);  // release: the buffer writes precede it
+      return true;
+    };
+    bool go = true;
+    for (uint64_t i = 0; i < cnt && go && !*abort_flag; ++i) {
+      go = drain(0, i);
+      if (go && i >= 1) go = drain(1, i - 1);
+    }
+    if (go && cnt > 0 && !*abort_flag) drain(1, cnt - 1);
+  } else if (warp == 16 && lane == 0) {
+    // ---- MMA issue
+    const uint32_t idesc = tc::idesc_bf16_f32(128, uint32_t(N));
+    const int nprod = P.precision == 1 ? 1 : 3;
+    uint64_t last2 = 0;
+    bool any2 = false;
+    auto issue = [&](int s2, uint64_t i) -> bool {
+      const int b = int(i & 1);
+      uint64_t* full = s2 == 0 ? &bfull1[b] : &bfull2[b];
+      if (!tc::mbar_wait(full, ph(i), kWaitLimit) ||
+          (i >= 2 && !tc::mbar_wait(&tfree[2 * s2 + b], ph(i - 2), kWaitLimit))) {
+        fail();
+        return false;
+      }
+      tc::tc_fence_after();
+      const uint32_t a0 = tc::smem_u32(sA + size_t(s2) * kFusedABytes);
+      const uint32_t bhs = tc::smem_u32(sB + size_t(b) * T * 8), bls = bhs + bbytes;
+      const uint32_t d = acc(s2, b);
+      uint32_t accum = 0;
+      for (int prod = 0; prod < nprod; ++prod) {
+        const uint32_t abase = a0 + (prod == 2 ? uint32_t(kFusedABytes / 2) : 0u);
+        const uint32_t bbase = prod == 1 ? bls : bhs;
+        for (int k = 0; k < 8; ++k) {
+          const uint64_t ad = tc::smem_desc(abase + uint32_t(k) * 2u * 2048u, 2048u, 128u);
+          const uint64_t bd = tc::smem_desc(bbase + uint32_t(k) * 2u * bk, bk, 128u);
+          tc::mma_bf16(d, ad, bd, idesc, accum);
+          accum = 1;
+        }
+      }
+      tc::mma_commit(&mdone[2 * s2 + b]);
+      if (s2 == 1) {
+        tc::mma_commit(&bfree[b]);  // buffer b may take tile i + 2
+        last2 = i;
+        any2 = true;
+      }
+      return true;
+    };
+    bool go = true;
+    for (uint64_t i = 0; i < cnt && go && !*abort_flag; ++i) {
+      go = issue(0, i);
+      if (go && i >= 1) go = issue(1, i - 1);
+    }
+    if (go && cnt > 0 && !*abort_flag) issue(1, cnt - 1);
+    // the last committed MMAs complete before TMEM is released
+    if (any2) tc::mbar_wait(&mdone[2 + int(last2 & 1)], ph(last2), kWaitLimit);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 4 * 64);
+}
+
 }  // namespace
 
 // one unitary per pass: 0 direct, 1 warp-specialised, 2 bulk-loaded (default)
@@ -1041,6 +1364,29 @@ int launch_fused(void* amp, const FusedPass& P, const void* d_a, int* d_err, cud
     k4_bulk<<<bgrid, kBulkThreads, bsmem, s>>>(static_cast<float2*>(amp), P,
                                                static_cast<const uint8_t*>(d_a), d_err, chunk_bits,
                                                lgb);
+    HS_CUDA(cudaGetLastError());
+    return HS_OK;
+  }
+  // two unitaries per pass on 2^12 tiles: both parts must meet the bulk
+  // form's conditions (slot 0 is tile bit 0, and a part holding it has it as
+  // local bit 0)
+  bool bulk2 = P.nops == 2 && P.m <= kBulk2MaxTileBits && P.m >= kFusedBits + 4 && P.tile.n > 0 &&
+               P.tile.src[0] == 0 && P.tile.dst[0] == 0 && P.tile.len[0] >= 2 &&
+               g_k4_variant.load() == 2;
+  for (int o = 0; o < 2; ++o)
+    for (int j = 1; j < kFusedBits; ++j) bulk2 = bulk2 && P.pbits[o][j] != 0;
+  if (bulk2) {
+    HS_TRY(smem_optin(reinterpret_cast<const void*>(k4_bulk2)));
+    const int chunk_bits = std::min<int>(P.tile.len[0], kBulkMaxChunkBits);
+    const int nchunks = T >> chunk_bits;
+    const size_t smem2 = 2 * size_t(kFusedABytes) + size_t(T) * 16 + size_t(nchunks) * 8 +
+                         64 * 8 + size_t(N) * 8 + 128 * 4 + size_t(2 * N + (N & 1)) * 4 +
+                         20 * 8 + 8 * kBulkStageFloats * 4;
+    if (smem2 > 227 * 1024) return set_error(HS_E_UNSUPPORTED, "K4 two-unitary pass needs %zu B", smem2);
+    const int sms = device_sms();
+    const int grid2 = int(P.ntiles < uint64_t(sms) ? P.ntiles : uint64_t(sms));
+    k4_bulk2<<<grid2, kBulk2Threads, smem2, s>>>(static_cast<float2*>(amp), P,
+                                                 static_cast<const uint8_t*>(d_a), d_err, chunk_bits);
     HS_CUDA(cudaGetLastError());
     return HS_OK;
   }

@@ -195,6 +195,24 @@ def propose(gates: Sequence[Gate], n: int, model: Optional[CostModel], dtype: in
             "candidates": {c: v[0] for c, v in cands.items()}}
 
 
+def propose_fewest(gates: Sequence[Gate], n: int, dtype: int = abi.C64, max_qubits: int = 12,
+                   max_len: int = 64) -> dict:
+    """The proposer's dynamic program with a trivial cost (every segment costs
+    1: the fewest parts) over the same orders and segment limits: the method
+    without the network, for measuring what the network adds."""
+    best = None
+    orders = {"dfs": partition.dfs_order(gates), "listed": list(range(len(gates)))}
+    for name, order in orders.items():
+        st, ln, _ = abi.order_segments(n, gates, order, max_qubits, max_len, dtype)
+        cuts, total = _dp(st, ln, np.ones(len(st)), len(order))
+        if cuts is None:
+            continue
+        parts = [[order[i] for i in range(a, a + l)] for a, l in cuts]
+        if best is None or total < best[0]:
+            best = (total, parts, f"fewest parts over {name} order")
+    return {"parts": best[1], "method": best[2], "num_parts": int(best[0])}
+
+
 def measure(st: "abi.State", gates: Sequence[Gate], parts, reps: int = 3, warmup: int = 1) -> float:
     """Device time (s) of one run of the circuit in the given parts (median)."""
     rec, offs = part_offsets(partition.parts_to_gates(gates, parts))

@@ -186,3 +186,23 @@ def test_k4_variants(port, variant, bits, n):
         abi.set_fused_shape(shape // 100, shape % 100)
     assert 1 - fid(want, got) <= 1e-8
     assert np.abs(got - want).max() <= 1e-5
+
+
+@pytest.mark.parametrize("n", [12, 14, 17, 20])
+def test_two_unitaries_per_pass(port, n):
+    """Two fused unitaries per state pass on 2^12 tiles (the first product
+    goes back to the tile's shared buffer and feeds the second on chip):
+    DFS-order parts of a U3 + CZ circuit against the oracle."""
+    gates = circuits.random_u3_cz(n, 10, 300 + n)
+    parts = partition.partition_dfs(gates, 6)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    prev = abi.set_fused_shape(2, 12)
+    try:
+        st = abi.State(n, abi.C64)
+        st.run_fused(rec, offs, 0)
+        got = st.amplitudes().astype(complex)
+    finally:
+        abi.set_fused_shape(prev // 100, prev % 100)
+    assert 1 - fid(want, got) <= 1e-8
+    assert np.abs(got - want).max() <= 1e-5
