@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--batch-check", type=int, default=512,
                     help="instances whose <H_C> is checked against complex128 plain runs")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned form")
+    ap.add_argument("--no-config1", action="store_true", help="skip the 30-qubit QFT section")
+    ap.add_argument("--config1-qubits", type=int, default=30)
     ap.add_argument("--learned-qubits", type=int, default=34)
     ap.add_argument("--learned-parts", type=int, default=20000, help="part timings harvested")
     return ap.parse_args()
@@ -410,6 +412,72 @@ def learned_form(args, abi, pg, device):
             "clocks": clk.summary()}
 
 
+def config1_form(args, abi, peak_gbs, pg, device):
+    """Config 1: the 30-qubit QFT (H, controlled phases 2 pi / 2^m on every
+    pair, final swaps) on a seeded random basis state, complex128, DFS-order
+    parts of <= 7 qubits: circuit time, passes and the K1 pass roofline.  And
+    the choice the plain path makes for parts on high qubits: a part whose
+    qubits are the top ones runs on strided tiles in one pass; the
+    alternative, a K2 bit-swap pass that brings those qubits to the low
+    slots followed by the part on contiguous tiles, is timed beside it."""
+    from hisvsim_b200 import circuits, partition
+    from hisvsim_b200.gates import Gate, part_offsets, to_records
+
+    n = args.config1_qubits
+    gates, x = circuits.qft(n, args.seed)
+    parts = partition.partition_dfs(gates, 7)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    st = abi.State(n, abi.C128)
+
+    def step():
+        st.set_basis(x)
+        st.run_parts(rec, offs)
+
+    t, c, clk = timed_steps(abi, step, max(1, args.warmup), max(1, args.steps), pg, device)
+    passes = c["passes"] / max(1, args.steps)
+    k1_ms = c["apply_us"] / 1e3 / max(1, c["passes"])
+    bpp = 2.0 * (1 << n) * 16
+    # a 7-qubit part of dense gates on the top qubits vs the same part on the
+    # lowest qubits after a bit-swap pass
+    rng = np.random.default_rng(7)
+    def part_on(qs):
+        g = []
+        for _ in range(2):
+            for q in qs:
+                g.append(Gate("U3", (q,), params=tuple(rng.uniform(0, 2 * np.pi, 3))))
+            for a, b in zip(qs[::2], qs[1::2]):
+                g.append(Gate("Z", (b,), (a,)))
+        return to_records(g)
+    hi = list(range(n - 7, n))
+    lo = list(range(2, 9))
+    r_hi, r_lo = part_on(hi), part_on(lo)
+    def dev_ms(fn, reps=5):
+        fn()
+        abi.synchronize()
+        a, b = abi.Event(), abi.Event()
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        return a.elapsed_ms(b) / reps
+    ms_hi = dev_ms(lambda: st.run_part(r_hi))
+    ms_lo = dev_ms(lambda: st.run_part(r_lo))
+    pairs = [(hi[i], lo[i]) for i in range(7)]
+    ms_swap = dev_ms(lambda: st.permute_bits(pairs[:5]), reps=4)
+    st.close()
+    return {"workload": f"QFT {n} qubits on a random basis state, {len(gates)} gates, "
+                        f"{len(parts)} DFS-order parts of <= 7 qubits, complex128",
+            "circuit_s": t, "passes_per_step": passes, "value": len(gates) * float(1 << n) / t,
+            "unit": UNIT,
+            "roofline": {"bound": "hbm", "kernel": "k1_part", "avg_launch_ms": k1_ms,
+                         "achieved": bpp / (k1_ms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
+                         "frac": bpp / (k1_ms / 1e3) / 1e9 / peak_gbs},
+            "high_qubit_parts": {"part_on_top_qubits_ms": ms_hi, "part_on_low_qubits_ms": ms_lo,
+                                 "bitswap_pass_5_pairs_ms": ms_swap,
+                                 "strided_tile_wins_by_ms": ms_lo + ms_swap - ms_hi},
+            "clocks": clk}
+
+
 def timed_steps(abi, step, warmup, steps, pg, device):
     """W untimed steps, then K steps between events on the library stream."""
     for _ in range(warmup):
@@ -516,6 +584,20 @@ def main():
 
     t_step, c, clk = timed_steps(abi, step, args.warmup, args.steps, pg, local)
     pbytes = abi.launch_bytes()
+    # the same circuit in parts of <= 10 qubits (2^12-amplitude tiles): fewer,
+    # longer passes
+    alt = None
+    if args.part_qubits == 9:
+        g10, p10, rec10, offs10 = workload(n, args.layers, args.seed + rank, 10, partitioner(args))
+
+        def step10():
+            st.set_basis(0)
+            st.run_parts(rec10, offs10)
+
+        t10, c10, _ = timed_steps(abi, step10, 1, 1, pg, local)
+        alt = {"part_qubits": 10, "parts": len(p10), "circuit_s": t10,
+               "value": world * upd / t10, "passes_per_step": c10["passes"],
+               "avg_launch_ms": c10["apply_us"] / 1e3 / max(1, c10["passes"])}
     passes = c["passes"] / args.steps
     k1_avg_ms = c["apply_us"] / 1e3 / max(1, c["passes"])
     bytes_per_pass = 2.0 * (1 << n) * 16
@@ -535,10 +617,11 @@ def main():
         traffic = tr.get("bytes_per_launch_scaled")
     except Exception:
         pass
-    # FP64 work of the plain pass: 8 FMA per amplitude for every dense
-    # one-qubit gate (U3), none for the CZ sign flips
+    # FP64 work of the plain pass: every U3 runs as a rotation of 9 FMA per
+    # amplitude pair (RY as two real plane rotations of 3 shears, the phase
+    # of the pair's second amplitude as 3 shears), the CZ sign flips take none
     dense = sum(1 for g in gates if g.name == "U3")
-    fma_step = dense * 8.0 * float(1 << n)
+    fma_step = dense * 4.5 * float(1 << n)
     fp64_peak = abi.fp64_peak_tflops()
     k1_total_s = c["apply_us"] / 1e6 / args.steps
     fp64 = {"fma_per_step": fma_step, "achieved_tflops": 2 * fma_step / k1_total_s / 1e12,
@@ -602,6 +685,10 @@ def main():
                        "-> norm readback (gate programs travel as kernel parameters; the "
                        "initial state |0..0> is created on the device, as StateVector does)"}
 
+    config1 = None
+    if not args.no_config1:
+        config1 = config1_form(args, abi, peak_gbs, pg, local)
+
     batch = None
     if not args.no_batch:
         batch = batch_form(args, abi, peak_gbs, pg, local)
@@ -640,8 +727,10 @@ def main():
                          "frac": k1_gbs / peak_gbs, "traffic": traffic, "peak_source": peak_src,
                          "kernel": "k1_part", "algorithmic_bytes_per_launch": bytes_per_pass,
                          "avg_launch_ms": k1_avg_ms, "fp64": fp64},
+            "parts_of_10_qubits": alt,
             "fused": fused,
             "redistribution": k2,
+            "config1": config1,
             "batch": batch,
             "learned": learned_res,
             "gpu_launches": int(c["passes"] + args.steps),

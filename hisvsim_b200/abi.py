@@ -17,7 +17,9 @@ import numpy as np
 from .gates import HS_GATE_DTYPE, Gate, to_records
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhisv.so")
+# HISV_LIB selects another build of the same library (the index-checked
+# libhisv_bounds.so next to it); the default is the normal build
+LIB_PATH = os.environ.get("HISV_LIB") or os.path.join(HERE, "libhisv.so")
 
 HS_OK = 0
 HS_E_INVALID = -1
@@ -80,6 +82,7 @@ SIGNATURES = {
     "hs_batch_tile_caps": [_vp, _vp],
     "hs_batch_state": [_vp, _i, _vp],
     "hs_batch_set_wait_limit": [_vp, _u32],
+    "hs_bounds_status": [_vp, _i],
     "hs_batch_block_step": [_vp, _i, _i, _i],
     "hs_batch_destroy": [_vp],
     "hs_mlp_create": [_i, ctypes.c_uint64, ctypes.POINTER(_vp)],
@@ -592,6 +595,13 @@ def set_k1_reg_bits(r: int) -> int:
     if rc < 0:
         check(rc)
     return rc
+
+
+def bounds_status(reset: bool = False) -> int:
+    """Kernel bits whose index checks failed (index-checked build only)."""
+    f = _u32(0)
+    check(lib().hs_bounds_status(ctypes.byref(f), int(reset)))
+    return f.value
 
 
 def counters():

@@ -73,6 +73,33 @@ def build_lib(verbose=False):
     return LIB
 
 
+BOUNDS_BUILD = os.path.join(HERE, "_build_bounds")
+BOUNDS_LIB = os.path.join(HERE, "libhisv_bounds.so")
+
+
+def build_bounds_lib(verbose=False):
+    """The same library with index checks at every kernel memory access
+    (-DHS_BOUNDS): libhisv_bounds.so, loaded through HISV_LIB by the
+    bounds tests."""
+    os.makedirs(BOUNDS_BUILD, exist_ok=True)
+    objs = []
+    hdrs = _headers()
+    for src in lib_sources():
+        obj = os.path.join(BOUNDS_BUILD, os.path.basename(src) + ".o")
+        if _stale(obj, [src] + hdrs):
+            cmd = [NVCC] + NVFLAGS + ["-DHS_BOUNDS"]
+            if src.endswith(".cpp"):
+                cmd += ["-x", "cu"]
+            cmd += ["-c", src, "-o", obj]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+        objs.append(obj)
+    if _stale(BOUNDS_LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", BOUNDS_LIB] + objs + ["-lcuda"])
+    return BOUNDS_LIB
+
+
 def pymod_path():
     return os.path.join(HERE, PYMOD_NAME + sysconfig.get_config_var("EXT_SUFFIX"))
 
@@ -98,6 +125,7 @@ def build_pymod(verbose=False):
 def build_all(verbose=False):
     build_lib(verbose)
     build_pymod(verbose)
+    build_bounds_lib(verbose)
 
 
 if __name__ == "__main__":

@@ -11,6 +11,7 @@
 #include <random>
 #include <set>
 
+#include "bounds.cuh"
 #include "internal.h"
 
 namespace hisv {
@@ -544,6 +545,20 @@ int hs_project(hs_state* st, const int32_t* qubits, const int32_t* values, int c
   if (prob_out) *prob_out = p;
   *out = ns;
   return HS_OK;
+}
+
+int hs_bounds_status(uint32_t* flags, int reset) {
+  if (!flags) return set_error(HS_E_INVALID, "null output");
+  *flags = 0;
+#ifdef HS_BOUNDS
+  HS_CUDA(cudaDeviceSynchronize());
+  *flags = bounds_take_part(reset) | bounds_take_misc(reset) | bounds_take_fused(reset) |
+           bounds_take_batch(reset);
+  return HS_OK;
+#else
+  (void)reset;
+  return set_error(HS_E_UNSUPPORTED, "this library was built without index checks");
+#endif
 }
 
 int hs_fp64_peak(double* tflops) {

@@ -18,6 +18,7 @@
 // with both ends in the tile (a table per phase pass), C the edges outside it
 // plus the crossing edges whose outer end is 1, and w_b = (#crossing edges
 // at tile bit b whose outer end is 0) - (#those whose outer end is 1).
+#include "bounds.cuh"
 #include "internal.h"
 
 namespace hisv {
@@ -203,7 +204,9 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
     {
       const uint64_t gb = bdep(t_begin, P.outer) + gt;
       for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads)
-        cp16(tiles_s + bswz(2u * uint32_t(c)) * 8u, amp + gb + S.gk[k]);
+        if (HS_IN_BOUNDS(gb + S.gk[k] + 2 <= (1ull << I.n) && bswz(2u * uint32_t(c)) + 2 <= uint32_t(T),
+                         kBoundsK6))
+          cp16(tiles_s + bswz(2u * uint32_t(c)) * 8u, amp + gb + S.gk[k]);
       cp_commit();
     }
     for (uint32_t ti = t_begin; ti < t_end; ++ti) {
@@ -220,7 +223,9 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
         const uint64_t nb = bdep(ti + 1, P.outer) + gt;
         const uint32_t ns = tiles_s + uint32_t((buf ^ 1) * kTileMax * 8);
         for (int k = 0, c = t; c < T / 2; ++k, c += kBatchThreads)
-          cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nb + S.gk[k]);
+          if (HS_IN_BOUNDS(nb + S.gk[k] + 2 <= (1ull << I.n) && bswz(2u * uint32_t(c)) + 2 <= uint32_t(T),
+                           kBoundsK6))
+            cp16(ns + bswz(2u * uint32_t(c)) * 8u, amp + nb + S.gk[k]);
         cp_commit();
       }
       for (int vi = 0; vi < nv; ++vi) {
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
               if ((e >> j) & 1) a ^= so[j];
-            v[e] = tile[a];
+            if (HS_IN_BOUNDS(a < uint32_t(T), kBoundsK6)) v[e] = tile[a];
           }
           // mixer RX(2 beta) = [[c, -i s], [-i s, c]] on register bit j
           auto rx_bit = [&](int j, float2 rx) {
@@ -291,6 +296,10 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
                     idx |= rb[j];
                     cc += wr[j];
                   }
+                if (!HS_IN_BOUNDS(idx < uint32_t(T) && int(S.cut[idx]) + cc >= 0 &&
+                                      int(S.cut[idx]) + cc <= nedges,
+                                  kBoundsK6))
+                  continue;
                 const float2 ph = S.phase[int(S.cut[idx]) + cc];
                 const float2 a = v[e];
                 v[e] = make_float2(ph.x * a.x - ph.y * a.y, ph.x * a.y + ph.y * a.x);
@@ -312,7 +321,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
 #pragma unroll
               for (int j = 0; j < 4; ++j)
                 if ((e >> j) & 1) off += ro[j];
-              base[off] = v[e];
+              if (HS_IN_BOUNDS(gbase + gl_base + off < (1ull << I.n), kBoundsK6)) base[off] = v[e];
             }
           } else {
 #pragma unroll
@@ -321,7 +330,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 6 : 3)
 #pragma unroll
               for (int j = 0; j < 4; ++j)
                 if ((e >> j) & 1) a ^= so[j];
-              tile[a] = v[e];
+              if (HS_IN_BOUNDS(a < uint32_t(T), kBoundsK6)) tile[a] = v[e];
             }
           }
         }
@@ -419,6 +428,10 @@ int max_ctas() {
   return n < 1 ? 1 : n;
 }
 }  // namespace
+
+#ifdef HS_BOUNDS
+HS_BOUNDS_TAKE(bounds_take_batch)
+#endif
 
 int batch_max_ctas_per_sm(int threads) {
   return threads == 256 ? max_ctas<256>() : max_ctas<128>();

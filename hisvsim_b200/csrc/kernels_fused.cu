@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 
+#include "bounds.cuh"
 #include "internal.h"
 #include "tcgen05.cuh"
 
@@ -832,8 +833,12 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
       __syncwarp();
       const float2* base = sv + dep(tile_of(i), P.outer);
       const uint32_t dst = tc::smem_u32(sB + size_t(b) * T * 8);
+      const uint64_t tb0 = dep(tile_of(i), P.outer);
       for (int c = lane; c < nchunks; c += 32)
-        tc::bulk_load(dst + uint32_t(c) * chunk_bytes, base + gc[c], chunk_bytes, &rfull[b]);
+        if (HS_IN_BOUNDS(tb0 + gc[c] + (chunk_bytes >> 3) <= (1ull << P.n) &&
+                             uint64_t(c + 1) * chunk_bytes <= uint64_t(T) * 8u,
+                         kBoundsK4))
+          tc::bulk_load(dst + uint32_t(c) * chunk_bytes, base + gc[c], chunk_bytes, &rfull[b]);
       issued = i + 1;
     }
     // no copy may still be landing when the CTA leaves: wait for the last
@@ -857,6 +862,7 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
         const int kb = item >> lgN, nn = item & (N - 1);
         const uint32_t tcol = tn[nn];
         const uint4 tp = *reinterpret_cast<const uint4*>(tq + 4 * kb);  // p = 4kb..4kb+3
+        if (!HS_IN_BOUNDS(((tp.x | tp.y | tp.z | tp.w) | tcol) < uint32_t(T), kBoundsK4)) continue;
         x[k][0] = *reinterpret_cast<const float2*>(buf + size_t(tp.x | tcol) * 8);
         x[k][1] = *reinterpret_cast<const float2*>(buf + size_t(tp.y | tcol) * 8);
         x[k][2] = *reinterpret_cast<const float2*>(buf + size_t(tp.z | tcol) * 8);
@@ -932,7 +938,8 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
           for (int s4 = 0; s4 < 4; ++s4) {
             const int p = (lane >> 3) + 4 * s4, c = 2 * (lane & 7);
             const float4 v = *reinterpret_cast<const float4*>(stg + sidx(p, c));
-            __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]), v);
+            if (HS_IN_BOUNDS(uint64_t(tb - sv) + gpq[p] + gn[c0 + c] + 2 <= (1ull << P.n), kBoundsK4))
+              __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]), v);
           }
         } else {
 #pragma unroll
@@ -940,8 +947,9 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
             const int p = 2 * ((lane >> 4) + 2 * s4), c = lane & 15;
             const float2 lo = *reinterpret_cast<const float2*>(stg + sidx(p, c));
             const float2 hi = *reinterpret_cast<const float2*>(stg + sidx(p + 1, c));
-            __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]),
-                   make_float4(lo.x, lo.y, hi.x, hi.y));
+            if (HS_IN_BOUNDS(uint64_t(tb - sv) + gpq[p] + gn[c0 + c] + 2 <= (1ull << P.n), kBoundsK4))
+              __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]),
+                     make_float4(lo.x, lo.y, hi.x, hi.y));
           }
         }
       }
@@ -1120,7 +1128,9 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
         const int per_chunk = int(chunk_bytes >> 4);  // 16-byte pieces per run
         for (int u = lane; u < (T >> 1); u += 32) {
           const int c = u / per_chunk, w = u - c * per_chunk;
-          cp_async16(dst + uint32_t(u) * 16u, base + gc[c] + 2 * w);
+          if (HS_IN_BOUNDS(dep(tile_of(i), P.outer) + gc[c] + 2 * w + 2 <= (1ull << P.n),
+                           kBoundsK4))
+            cp_async16(dst + uint32_t(u) * 16u, base + gc[c] + 2 * w);
         }
         asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
                          tc::smem_u32(&rfull[b]))
@@ -1128,8 +1138,12 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
       } else {
         if (lane == 0) tc::mbar_arrive_expect_tx(&rfull[b], uint32_t(T) * 8u);
         __syncwarp();
+        const uint64_t tb0 = dep(tile_of(i), P.outer);
         for (int c = lane; c < nchunks; c += 32)
-          tc::bulk_load(dst + uint32_t(c) * chunk_bytes, base + gc[c], chunk_bytes, &rfull[b]);
+          if (HS_IN_BOUNDS(tb0 + gc[c] + (chunk_bytes >> 3) <= (1ull << P.n) &&
+                               uint64_t(c + 1) * chunk_bytes <= uint64_t(T) * 8u,
+                           kBoundsK4))
+            tc::bulk_load(dst + uint32_t(c) * chunk_bytes, base + gc[c], chunk_bytes, &rfull[b]);
       }
       issued = i + 1;
     }
@@ -1156,6 +1170,7 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
         const int kb = item >> lgN, nn = item & (N - 1);
         const uint32_t tcol = tns[nn];
         const uint4 tp = *reinterpret_cast<const uint4*>(tqs + 4 * kb);
+        if (!HS_IN_BOUNDS(((tp.x | tp.y | tp.z | tp.w) | tcol) < uint32_t(T), kBoundsK4)) continue;
         x[k][0] = *reinterpret_cast<const float2*>(buf + size_t(tp.x | tcol) * 8);
         x[k][1] = *reinterpret_cast<const float2*>(buf + size_t(tp.y | tcol) * 8);
         x[k][2] = *reinterpret_cast<const float2*>(buf + size_t(tp.z | tcol) * 8);
@@ -1246,10 +1261,13 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
             const float2 hi = *reinterpret_cast<const float2*>(stg + sidx(p + 1, c));
             v = make_float4(lo.x, lo.y, hi.x, hi.y);
           }
-          if (to_smem)
-            *reinterpret_cast<float4*>(sbuf + (tqs[p] | tns[c0 + c])) = v;
-          else
+          if (to_smem) {
+            if (HS_IN_BOUNDS((tqs[p] | tns[c0 + c]) + 2u <= uint32_t(T), kBoundsK4))
+              *reinterpret_cast<float4*>(sbuf + (tqs[p] | tns[c0 + c])) = v;
+          } else if (HS_IN_BOUNDS(uint64_t(tb - sv) + gpq[p] + gn2[c0 + c] + 2 <= (1ull << P.n),
+                                  kBoundsK4)) {
             __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn2[c0 + c]), v);
+          }
         }
       }
       tc::tc_fence_before();
@@ -1315,6 +1333,10 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
 }
 
 }  // namespace
+
+#ifdef HS_BOUNDS
+HS_BOUNDS_TAKE(bounds_take_fused)
+#endif
 
 // one unitary per pass: 0 direct, 1 warp-specialised, 2 bulk-loaded (default)
 std::atomic<int> g_k4_variant{2};

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "bounds.cuh"
 #include "internal.h"
 
 namespace hisv {
@@ -355,12 +356,14 @@ __global__ void __launch_bounds__(kK2Threads) k2_tile(V* __restrict__ sv, const 
   const bool active = t < T;
   const uint64_t gt = dep_runs(uint64_t(t), P.tile);
   const uint32_t sb = uint32_t(__cvta_generic_to_shared(bufs));
+  const uint64_t size = P.ntiles << P.m;  // amplitudes of the state (bounds checks)
   auto issue = [&](uint64_t tile, int b) {
     if (!active) return;
     const uint64_t gb = dep_runs(tile, P.outer) + gt;
     for (int k = 0; k < per; ++k) {
       const uint32_t j = uint32_t(t + k * kK2Threads);
-      cp_async_el<sizeof(V)>(sb + uint32_t((b * T + j) * sizeof(V)), sv + gb + gk[k]);
+      if (HS_IN_BOUNDS(gb + gk[k] < size && j < uint32_t(T), kBoundsK2))
+        cp_async_el<sizeof(V)>(sb + uint32_t((b * T + j) * sizeof(V)), sv + gb + gk[k]);
     }
   };
   uint64_t tile = blockIdx.x;
@@ -381,7 +384,8 @@ __global__ void __launch_bounds__(kK2Threads) k2_tile(V* __restrict__ sv, const 
           const uint32_t d = ((j >> P.pa[i]) ^ (j >> P.pb[i])) & 1u;
           j ^= d * ((1u << P.pa[i]) | (1u << P.pb[i]));
         }
-        __stcs(sv + gb + gk[k], cur[j]);
+        if (HS_IN_BOUNDS(gb + gk[k] < size && j < uint32_t(T), kBoundsK2))
+          __stcs(sv + gb + gk[k], cur[j]);
       }
     }
     __syncthreads();  // this buffer is refilled by the prefetch issued next iteration
@@ -442,6 +446,10 @@ int launch_tile_perm(V* amp, int n, const int32_t* pairs, int np, int max_bits, 
   return HS_OK;
 }
 }  // namespace
+
+#ifdef HS_BOUNDS
+HS_BOUNDS_TAKE(bounds_take_misc)
+#endif
 
 int launch_permute(void* amp, int dtype, int n, const int32_t* pairs, int npairs,
                    cudaStream_t s) {

@@ -17,6 +17,7 @@
 // Op dispatch: every op carries one dense code (K1Code), so the switch below
 // is a jump table; op descriptors are read from the (warp-uniform) parameter
 // space, coefficients from a shared-memory copy (one 16-byte load each).
+#include "bounds.cuh"
 #include "internal.h"
 
 namespace hisv {
@@ -267,6 +268,7 @@ __device__ __forceinline__ void run_op(V (&v)[1 << R], const DevOp& op, const do
   const uint64_t w0 = ow[0], w1 = ow[1], w2 = ow[2];
   const int code = int(w0 >> 8) & 255;
   const double2* c = s_coef + (uint32_t(w1) & 0xffffu);
+  if (!HS_IN_BOUNDS((uint32_t(w1) & 0xffffu) <= uint32_t(P.ncoef), kBoundsK1)) return;
   const uint32_t cthr = uint32_t(w1 >> 32);
   // thread and outer part of the controls (the register part is in the code /
   // creg); evaluated only by the ops that have such controls
@@ -359,9 +361,16 @@ template <typename V>
 __device__ __forceinline__ void issue_tile_load(const V* __restrict__ sv, uint32_t sbuf,
                                                 uint64_t gbase, const uint64_t* __restrict__ gchunk,
                                                 const uint32_t* __restrict__ cswz, uint32_t tswz,
-                                                uint64_t gt, int nchunk_per_thr) {
+                                                uint64_t gt, int nchunk_per_thr, uint64_t size,
+                                                uint32_t tile_bytes) {
   const V* base = sv + gbase + gt;
-  for (int k = 0; k < nchunk_per_thr; ++k) cp_async16(sbuf + (tswz ^ cswz[k]), base + gchunk[k]);
+  for (int k = 0; k < nchunk_per_thr; ++k)
+    if (HS_IN_BOUNDS(gbase + gt + gchunk[k] + 16 / sizeof(V) <= size &&
+                         (tswz ^ cswz[k]) + 16u <= tile_bytes,
+                     kBoundsK1))
+      cp_async16(sbuf + (tswz ^ cswz[k]), base + gchunk[k]);
+  (void)size;
+  (void)tile_bytes;
 }
 
 // CTA shapes: 2^(m-R) threads.  Complex128 with 16 amplitudes per thread:
@@ -394,6 +403,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
   const uint32_t t = threadIdx.x;
   const uint32_t nthr = blockDim.x;
   const uint32_t tile_bytes = uint32_t(sizeof(V)) << P.m;
+  const uint64_t size = 1ull << P.n;  // amplitudes of the state (bounds checks)
   double2* s_coef = reinterpret_cast<double2*>(smem_raw + tile_bytes);
   uint64_t* s_gchunk = reinterpret_cast<uint64_t*>(s_coef + P.ncoef);
   // chunk c = t + k*nthr; its first tile index is c << SH.  The bits of t and
@@ -433,7 +443,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
   uint64_t tile = blockIdx.x;
   // global offset of the tile being processed (computed when its copy is issued)
   uint64_t gbase = tile < P.ntiles ? deposit(tile, P.outer) : 0;
-  if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, gbase, s_gchunk, s_cswz, tswz, gt, per_thr);
+  if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, gbase, s_gchunk, s_cswz, tswz, gt, per_thr, size, tile_bytes);
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
@@ -456,14 +466,16 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
         return d;
       };
 #pragma unroll
-      for (int e = 0; e < E; ++e) v[e] = *reinterpret_cast<const V*>(smem_raw + (a0 ^ ux(e)));
+      for (int e = 0; e < E; ++e)
+        if (HS_IN_BOUNDS((a0 ^ ux(e)) + sizeof(V) <= tile_bytes, kBoundsK1))
+          v[e] = *reinterpret_cast<const V*>(smem_raw + (a0 ^ ux(e)));
       if (last) {
         // every thread holds its registers of the last group: the buffer
         // takes the next tile while this one is finished and stored (one
         // tile buffer per CTA leaves room for more CTAs per SM)
         __syncthreads();
         if (next < P.ntiles) {
-          issue_tile_load<V>(sv, sb0, gnext, s_gchunk, s_cswz, tswz, gt, per_thr);
+          issue_tile_load<V>(sv, sb0, gnext, s_gchunk, s_cswz, tswz, gt, per_thr, size, tile_bytes);
           cp_async_commit();
         }
       }
@@ -476,7 +488,9 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
 #define SLOT(J)                                                             \
   if constexpr ((J) < R) {                                                  \
     if (mask & (1u << (J))) {                                               \
-      const double2* c = s_coef + (uint32_t(rw >> (24 + 10 * (J))) & 1023u); \
+      const uint32_t ci = uint32_t(rw >> (24 + 10 * (J))) & 1023u;          \
+      if (!HS_IN_BOUNDS(ci + 1u + ((zmask >> (J)) & 1u) <= uint32_t(P.ncoef), kBoundsK1)) continue; \
+      const double2* c = s_coef + ci;                                       \
       if (zmask & (1u << (J)))                                              \
         rot<R, (J), true>(v, c[0], c[1]);                                   \
       else                                                                  \
@@ -502,13 +516,15 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
             const int j = lowest_bit(i);
             if ((e >> j) & 1) p += s_glreg[j]; else p -= s_glreg[j];
           }
-          __stcs(p, v[e]);
+          if (HS_IN_BOUNDS(uint64_t(p - sv) < size, kBoundsK1)) __stcs(p, v[e]);
         }
         // the next tile's copies (the only ones in flight) must have landed
         cp_async_wait<0>();
       } else {
 #pragma unroll
-        for (int e = 0; e < E; ++e) *reinterpret_cast<V*>(smem_raw + (a0 ^ ux(e))) = v[e];
+        for (int e = 0; e < E; ++e)
+          if (HS_IN_BOUNDS((a0 ^ ux(e)) + sizeof(V) <= tile_bytes, kBoundsK1))
+            *reinterpret_cast<V*>(smem_raw + (a0 ^ ux(e))) = v[e];
       }
       __syncthreads();
     }
@@ -583,6 +599,10 @@ int launch_typed(V* a, const PartProgram& P, cudaStream_t s) {
   if (sizeof(V) == 16 && (P.m - P.rbits) > 7) return launch_shape<true>(a, P, s);
   return launch_shape<false>(a, P, s);
 }
+
+#ifdef HS_BOUNDS
+HS_BOUNDS_TAKE(bounds_take_part)
+#endif
 
 int launch_part(void* amp, int dtype, const PartProgram& P, cudaStream_t s) {
   if (P.ngroups < 1 || P.nops < 1) return HS_OK;

@@ -246,6 +246,15 @@ int hs_permute_bits(hs_state* st, const int32_t* pairs, int num_pairs, void* str
  * in-place involution passes of K2. */
 int hs_gather_qubits(hs_state* st, const int32_t* proc_qubits, int num, void* stream);
 
+/* ---- bounds-checked build (no counterpart in the reference) -----------------
+ * libhisv_bounds.so is this library compiled with index checks at every
+ * global and shared-memory access of the part (K1), bit-swap (K2), fused
+ * (K4) and batch (K6) kernels; a failed check skips the access and sets the
+ * kernel's bit (1 = K1, 2 = K2, 4 = K4, 8 = K6).  flags: the bits set since
+ * the last reset (synchronises the device).  The normal build returns
+ * HS_E_UNSUPPORTED. */
+int hs_bounds_status(uint32_t* flags, int reset);
+
 /* ---- FP64 reductions (K3) ------------------------------------------------- */
 
 /* sum |a|^2 (is_normalized, state_vector.hpp:63-72) */

@@ -237,3 +237,16 @@ def test_proposer_dp_and_fallback():
     cuts, total = learned._dp(np.array([0, 0, 1, 2]), np.array([1, 3, 2, 1]),
                               np.array([1.0, 2.5, 1.0, 1.0]), 3)
     assert cuts == [(0, 1), (1, 2)] and total == 2.0
+
+
+def test_index_checks_only_in_the_checked_build():
+    """The normal build has no index checks (hs_bounds_status says so); the
+    index-checked build exports the same C ABI."""
+    with pytest.raises(abi.HisvError) as e:
+        abi.bounds_status()
+    assert e.value.code == abi.HS_E_UNSUPPORTED
+    path = os.path.join(ROOT, "hisvsim_b200", "libhisv_bounds.so")
+    assert os.path.exists(path)
+    L = ctypes.CDLL(path)
+    missing = [n for n in header_functions() if not hasattr(L, n)]
+    assert not missing, missing
