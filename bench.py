@@ -420,6 +420,8 @@ def config1_form(args, abi, peak_gbs, pg, device):
     qubits are the top ones runs on strided tiles in one pass; the
     alternative, a K2 bit-swap pass that brings those qubits to the low
     slots followed by the part on contiguous tiles, is timed beside it."""
+    import numpy as np
+
     from hisvsim_b200 import circuits, partition
     from hisvsim_b200.gates import Gate, part_offsets, to_records
 
