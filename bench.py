@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -619,11 +620,14 @@ def main():
         traffic = tr.get("bytes_per_launch_scaled")
     except Exception:
         pass
-    # FP64 work of the plain pass: every U3 runs as a rotation of 9 FMA per
-    # amplitude pair (RY as two real plane rotations of 3 shears, the phase
-    # of the pair's second amplitude as 3 shears), the CZ sign flips take none
+    # FP64 work of the plain pass: every U3 runs as a rotation, per amplitude
+    # pair 3 FMA for the phase of the pair's second amplitude and 2 x 2 real
+    # shears for RY when |cos(theta/2)| >= 0.4 (the planner's two-shear form,
+    # its scale carried in the frames), else 2 x 3; the CZ sign flips take none
+    fma_pair = sum(3 + (4 if abs(math.cos(complex(g.params[0]).real / 2)) >= 0.4 else 6)
+                   for g in gates if g.name == "U3")
     dense = sum(1 for g in gates if g.name == "U3")
-    fma_step = dense * 4.5 * float(1 << n)
+    fma_step = fma_pair * 0.5 * float(1 << n)
     fp64_peak = abi.fp64_peak_tflops()
     k1_total_s = c["apply_us"] / 1e6 / args.steps
     fp64 = {"fma_per_step": fma_step, "achieved_tflops": 2 * fma_step / k1_total_s / 1e12,
@@ -718,7 +722,7 @@ def main():
                                    f"(U3 all qubits + CZ random matching), plain complex128",
                        "gates": len(gates), "parts": len(parts),
                        "part_qubits": args.part_qubits, "partitioner": args.partitioner,
-                       "tile_qubits": args.tile_qubits or "automatic (2^10 tiles, 8 amplitudes "
+                       "tile_qubits": args.tile_qubits or "automatic (2^10 tiles, 16 amplitudes "
                                                           "per thread for complex128)",
                        "passes_per_step": passes, "state_bytes": (1 << n) * 16,
                        "l2": "state >> L2 (126 MB), no flush", "parallelism": f"replicas{world}"},

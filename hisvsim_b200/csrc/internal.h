@@ -103,7 +103,7 @@ struct DevOp {
   uint32_t cthr;              // control/mask bits that are thread bits (tile-index space)
   uint64_t couter;            // control/mask bits outside the tile (global index space)
   uint16_t fl_first, fl_n;    // flush: entries [fl_first, fl_first + fl_n) of flw/flp
-  uint32_t pad;
+  uint32_t form;              // rotation: shear form (RoundDesc), else 0
 };
 static_assert(sizeof(DevOp) == 32, "DevOp layout");
 
@@ -117,19 +117,22 @@ struct Runs {  // bit-run deposit: out |= ((x >> src) & (2^len - 1)) << dst
 // A round of a register group, packed in one 64-bit word (read with a single
 // load): at most one rotation per register bit j, applied in the order
 // j = 0, 1, ..., then ops[others[first_other .. first_other + num_other)).
-//   bits  0- 3  rotation on register bit j present
-//   bits  4- 7  with a phase part
-//   bits  8-15  num_other
-//   bits 16-23  first_other
-//   bits 24+10j coefficient index of the rotation on bit j (coef[idx], [idx+1])
+//   bits  0- 3  rotation on register bit j has a phase part
+//   bits  4-11  num_other
+//   bits 12-19  first_other
+//   bits 20+11j rotation on register bit j: bits 0-8 coefficient pair p
+//               (coef[2p], coef[2p+1]; p = 0: no rotation), bits 9-10 its
+//               shear form: 0 three shears, 1 without the third, 2 without
+//               the first
 // The planner packs a group's ops into rounds without changing their order
 // where they do not commute.
 using RoundDesc = uint64_t;
-inline RoundDesc round_pack(uint32_t mask, uint32_t zmask, uint32_t first_other,
-                            uint32_t num_other, const uint32_t cidx[4]) {
-  uint64_t w = uint64_t(mask & 15u) | uint64_t(zmask & 15u) << 4 | uint64_t(num_other & 255u) << 8 |
-               uint64_t(first_other & 255u) << 16;
-  for (int j = 0; j < 4; ++j) w |= uint64_t(cidx[j] & 1023u) << (24 + 10 * j);
+inline RoundDesc round_pack(uint32_t zmask, uint32_t first_other, uint32_t num_other,
+                            const uint32_t pair[4], const uint32_t form[4]) {
+  uint64_t w = uint64_t(zmask & 15u) | uint64_t(num_other & 255u) << 4 |
+               uint64_t(first_other & 255u) << 12;
+  for (int j = 0; j < 4; ++j)
+    w |= uint64_t((pair[j] & 511u) | (form[j] & 3u) << 9) << (20 + 11 * j);
   return w;
 }
 
@@ -168,7 +171,7 @@ struct PartProgram {
   double2 coef[kMaxCoef];
 };
 static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");
-static_assert(kMaxOps <= 256 && kMaxCoef <= 1024, "round packing");
+static_assert(kMaxOps <= 256 && kMaxCoef <= 1024, "round packing: 8-bit op indices, 9-bit coefficient pairs");
 
 // Pending diagonal of a state under planning: the true state is
 // G * (prod_q diag(1, r[q]) on qubit q) * (the stored amplitudes).  Uncontrolled

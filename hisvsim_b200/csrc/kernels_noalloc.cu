@@ -22,7 +22,8 @@
 // keeps the last call's contents; each call writes every partial it reads and
 // the result slot before reading them, so nothing needs clearing between
 // calls.  Calls that overlap on the GPU (concurrent streams or threads) race
-// on the array and must be serialised by the caller.
+// on the array and must be serialised by the caller.  Every call copies the
+// result to the host and synchronises the given stream before it returns.
 #include <mutex>
 
 #include "internal.h"

@@ -104,18 +104,20 @@ __device__ __forceinline__ float flip_sign(float x, uint32_t sm) {
   return __int_as_float(__float_as_int(x) ^ int(sm));
 }
 
-// Rotation RY(theta) diag(1, e^{i beta}) on register bit J, every step an
-// in-place shear x += t y (so no register is copied): the phase turns the
-// (re, im) plane of the pair's second amplitude by beta, RY the (first,
-// second) plane of the real and of the imaginary parts by theta/2; a plane
-// rotation by w is the three shears x -= tan(w/2) y, y += sin(w) x,
-// x -= tan(w/2) y.  cy = (tan(theta/4), sin(theta/2)), cz = (tan(beta/2),
-// sin(beta)).  9 FMA per amplitude pair, 6 without the phase.
+// Rotation on register bit J, every step an in-place shear x += t y (so no
+// register is copied): with Z, the phase e^{i beta} turns the (re, im) plane
+// of the pair's second amplitude B by the three shears (cz = (tan(beta/2),
+// sin(beta))); then the (A.re, B.re) and (A.im, B.im) planes take the real
+// shears of cy = (t, s) in the given form: 0 = A += tB; B += sA; A += tB
+// (an exact plane rotation), 1 = the first two, 2 = the last two (the
+// planner carries the scale these leave).  9 FMA per amplitude pair (7 in
+// forms 1 and 2), 6 (4) without the phase.  The form is warp-uniform.
 template <int R, int J, bool Z, typename V>
-__device__ __forceinline__ void rot(V (&v)[1 << R], const double2 cy, const double2 cz) {
+__device__ __forceinline__ void rot(V (&v)[1 << R], const double2 cy, const double2 cz,
+                                    uint32_t form) {
   using T = typename Scalar<V>::T;
   constexpr int NP = (1 << R) / 2;
-  const T ty = T(cy.x), sy = T(cy.y), tz = T(cz.x), sz = T(cz.y);
+  const T t = T(cy.x), s = T(cy.y), tz = T(cz.x), sz = T(cz.y);
   // one shear at a time across all pairs: NP-fold independent FMAs per step
 #define A(p) v[ins0<J>(p)]
 #define B(p) v[ins0<J>(p) | (1 << J)]
@@ -127,20 +129,24 @@ __device__ __forceinline__ void rot(V (&v)[1 << R], const double2 cy, const doub
 #pragma unroll
     for (int p = 0; p < NP; ++p) B(p).x = fma(-tz, B(p).y, B(p).x);
   }
+  if (!(form & 2u)) {
 #pragma unroll
-  for (int p = 0; p < NP; ++p) {
-    A(p).x = fma(-ty, B(p).x, A(p).x);
-    A(p).y = fma(-ty, B(p).y, A(p).y);
+    for (int p = 0; p < NP; ++p) {
+      A(p).x = fma(t, B(p).x, A(p).x);
+      A(p).y = fma(t, B(p).y, A(p).y);
+    }
   }
 #pragma unroll
   for (int p = 0; p < NP; ++p) {
-    B(p).x = fma(sy, A(p).x, B(p).x);
-    B(p).y = fma(sy, A(p).y, B(p).y);
+    B(p).x = fma(s, A(p).x, B(p).x);
+    B(p).y = fma(s, A(p).y, B(p).y);
   }
+  if (!(form & 1u)) {
 #pragma unroll
-  for (int p = 0; p < NP; ++p) {
-    A(p).x = fma(-ty, B(p).x, A(p).x);
-    A(p).y = fma(-ty, B(p).y, A(p).y);
+    for (int p = 0; p < NP; ++p) {
+      A(p).x = fma(t, B(p).x, A(p).x);
+      A(p).y = fma(t, B(p).y, A(p).y);
+    }
   }
 #undef A
 #undef B
@@ -484,22 +490,23 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
       Deferred dfr;
       for (int r = G.first_round, r_end = G.first_round + G.num_rounds; r < r_end; ++r) {
         const uint64_t rw = P.rounds[r];
-        const uint32_t mask = uint32_t(rw) & 15u, zmask = (uint32_t(rw) >> 4) & 15u;
+        const uint32_t zmask = uint32_t(rw) & 15u;
 #define SLOT(J)                                                             \
   if constexpr ((J) < R) {                                                  \
-    if (mask & (1u << (J))) {                                               \
-      const uint32_t ci = uint32_t(rw >> (24 + 10 * (J))) & 1023u;          \
-      if (!HS_IN_BOUNDS(ci + 1u + ((zmask >> (J)) & 1u) <= uint32_t(P.ncoef), kBoundsK1)) continue; \
+    const uint32_t sw = uint32_t(rw >> (20 + 11 * (J))) & 2047u;            \
+    if (sw & 511u) {                                                        \
+      const uint32_t ci = (sw & 511u) * 2u;                                 \
+      if (!HS_IN_BOUNDS(ci + 2u <= uint32_t(P.ncoef), kBoundsK1)) continue; \
       const double2* c = s_coef + ci;                                       \
       if (zmask & (1u << (J)))                                              \
-        rot<R, (J), true>(v, c[0], c[1]);                                   \
+        rot<R, (J), true>(v, c[0], c[1], sw >> 9);                          \
       else                                                                  \
-        rot<R, (J), false>(v, c[0], c[0]);                                  \
+        rot<R, (J), false>(v, c[0], c[0], sw >> 9);                         \
     }                                                                       \
   }
         SLOT(0) SLOT(1) SLOT(2) SLOT(3)
 #undef SLOT
-        const int k0 = int(rw >> 16) & 255, k1 = k0 + (int(rw >> 8) & 255);
+        const int k0 = int(rw >> 12) & 255, k1 = k0 + (int(rw >> 4) & 255);
         for (int k = k0; k < k1; ++k) {
           run_op<R, FULL, FAST>(v, P.ops[P.others[k]], s_coef, thr, gbase, dfr, P);
         }

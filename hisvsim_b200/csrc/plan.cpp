@@ -29,8 +29,11 @@
 // second) plane of the pair's real and of its imaginary parts by theta/2.
 // 9 FP64 FMA per amplitude pair (6 without the phase), every one updating a
 // register in place, so the kernel's op dispatch needs no register moves.
-// diag(a0, a1) joins the pending diagonal, which commutes with every diagonal
-// gate (CZ, phases) and is absorbed by the next one-qubit gate on q.
+// For complex128 states the RY part is instead written, when cos(theta/2) >=
+// 0.4, as two shears and a real diagonal scale that joins the pending factor
+// (factor_rotation): 7 FMA per pair.  diag(a0, a1) (times that scale) joins
+// the pending diagonal, which commutes with every diagonal gate (CZ, phases)
+// and is absorbed by the next one-qubit gate on q.
 // Diagonal one-qubit gates (S, T, RZ, ...) only update the pending diagonal.
 // Whatever is pending at the end of a call is applied by one flush op.  The
 // result is the reference's state up to rounding.
@@ -80,32 +83,62 @@ bool is_diagonal(const LoweredGate& g) {
 }
 
 // ---- the factored rotation ---------------------------------------------------
+// Applied to the stored pair (A, B) = (amplitude with the qubit 0, with it 1):
+// first the phase b1 = e^{i beta} on B as the three shears of its (re, im)
+// plane (tan(beta/2), sin(beta)), then real shears on the (A.re, B.re) and
+// (A.im, B.im) planes with one coefficient pair (t, s):
+//   form 0:  A += t B;  B += s A;  A += t B
+//   form 1:  A += t B;  B += s A
+//   form 2:             B += s A;  A += t B
+// and the left diagonal diag(g0, g1) joins the pending factors.
 struct Rot {
   bool has_z;        // phase part present (beta != 0)
   double tz, sz;     // shears of the phase: tan(beta/2), sin(beta)
-  double ty, sy;     // shears of RY: tan(theta/4), sin(theta/2)
-  cplx a0, a1;       // left diagonal (the new pending diagonal of the qubit)
+  int form;
+  double t, s;
+  cplx g0, g1;       // left diagonal
 };
 
-// W = diag(a0, a1) * [[c, -s], [s, c]] * diag(1, b1), c = |W00|, s = |W10|
-// (c = cos(theta/2), s = sin(theta/2), theta in [0, pi]; b1 = e^{i beta}).
-// False when W is not unitary to 1e-12 (custom C1 matrices need not be).
-bool factor_rotation(const cplx* W, Rot* R) {
+// Two-shear forms are used when cos(theta/2) >= kShearPivot: their
+// coefficients stay below ~3 and the pending scale of a qubit within
+// [kShearPivot^2, kShearPivot^-2].
+constexpr double kShearPivot = 0.4;
+
+// W = U diag(1, r): U unitary, r the qubit's pending factor, so W's first
+// column is a unit vector and its second |r| = rho times one.  With
+// Wn = W diag(1, 1/rho) = diag(a0, a1) RY diag(1, b1) (Z-Y-Z; RY = [[c, -sg],
+// [sg, c]], c = cos(theta/2) >= 0, |arg b1| <= pi/2):
+//   W = diag(a0, a1) M diag(1, b1),  M = RY diag(1, rho) = [[c, -sg rho], [sg, c rho]],
+// and M is written as shears times a left diagonal:
+//   form 0 (exact rotation): M = diag(1, rho) S3, S3 the three shears with
+//     t = -rho tan(theta/4), s = sg / rho (rho never changes);
+//   form 1 (scaled, rho <= 1): M = diag(c, rho / c) [[1, 0], [s, 1]] [[1, t], [0, 1]],
+//     t = -sg rho / c, s = sg c / rho (rho grows to rho / c^2);
+//   form 2 (scaled, rho > 1): M = diag(1 / c, c rho) [[1, t], [0, 1]] [[1, 0], [s, 1]],
+//     s = sg / (c rho), t = -sg c rho (rho shrinks to c^2 rho).
+// Forms 1 and 2 take 4 FMA per pair instead of 6 and leave a real scale on
+// the qubit's two values, which complex128 frames carry (`scaled`);
+// complex64 states keep form 0.  False when W is not of the form above to
+// 1e-12 (custom C1 matrices need not be).
+bool factor_rotation(const cplx* W, bool scaled, Rot* R) {
   const double c = std::abs(W[0]), s = std::abs(W[2]);
-  const double c1 = std::abs(W[3]), s1 = std::abs(W[1]);
+  const double rho = std::hypot(std::abs(W[1]), std::abs(W[3]));
   const double tol = 1e-12;
+  if (!(rho > 0.0) || !std::isfinite(rho)) return false;
+  const cplx w1 = W[1] / rho, w3 = W[3] / rho;
+  const double c1 = std::abs(w3), s1 = std::abs(w1);
   if (std::fabs(c * c + s * s - 1.0) > tol || std::fabs(c1 * c1 + s1 * s1 - 1.0) > tol ||
-      std::abs(std::conj(W[0]) * W[1] + std::conj(W[2]) * W[3]) > tol)
+      std::abs(std::conj(W[0]) * w1 + std::conj(W[2]) * w3) > tol)
     return false;
   cplx a0, a1, b1;
   double cc = c, ss = s;
   if (c > 0.0 && s > 0.0) {
     a0 = W[0] / c;
     a1 = W[2] / s;
-    b1 = c >= s ? W[3] / (a1 * c) : -W[1] / (a0 * s);
+    b1 = c >= s ? w3 / (a1 * c) : -w1 / (a0 * s);
     b1 /= std::abs(b1);
   } else if (c == 0.0) {  // anti-diagonal
-    a0 = -W[1];
+    a0 = -w1;
     a1 = W[2];
     b1 = 1.0;
     cc = 0.0;
@@ -113,7 +146,7 @@ bool factor_rotation(const cplx* W, Rot* R) {
   } else {
     return false;  // diagonal: handled by the caller
   }
-  // the norms of the rows are 1 to 1e-12; keep the left diagonal unit-modulus
+  // the norms of the rows are 1 to 1e-12; keep the phases unit-modulus
   a0 /= std::abs(a0);
   a1 /= std::abs(a1);
   const double nrm = std::hypot(cc, ss);
@@ -126,11 +159,30 @@ bool factor_rotation(const cplx* W, Rot* R) {
     a1 = -a1;
     sign = -1.0;
   }
-  R->a0 = a0;
-  R->a1 = a1;
-  // tan(theta/4) = s / (1 + c) (half-angle formula for theta/2, c >= 0)
-  R->ty = sign * ss / (1.0 + cc);
-  R->sy = sign * ss;
+  const double sg = sign * ss;
+  double g0 = 1.0, g1 = rho;
+  if (scaled && cc >= kShearPivot) {
+    if (rho <= 1.0) {
+      R->form = 1;
+      R->t = -sg * rho / cc;
+      R->s = sg * cc / rho;
+      g0 = cc;
+      g1 = rho / cc;
+    } else {
+      R->form = 2;
+      R->s = sg / (cc * rho);
+      R->t = -sg * cc * rho;
+      g0 = 1.0 / cc;
+      g1 = cc * rho;
+    }
+  } else {
+    // tan(theta/4) = s / (1 + c) (half-angle formula for theta/2, c >= 0)
+    R->form = 0;
+    R->t = -rho * sg / (1.0 + cc);
+    R->s = sg / rho;
+  }
+  R->g0 = a0 * g0;
+  R->g1 = a1 * g1;
   R->has_z = !(b1.real() == 1.0 && b1.imag() == 0.0);
   // tan(beta/2) = sin(beta) / (1 + cos(beta)), cos(beta) >= 0
   R->tz = R->has_z ? b1.imag() / (1.0 + b1.real()) : 0.0;
@@ -188,7 +240,10 @@ RGate flush_gate(Frames* F) {
   return x;
 }
 
-void rewrite(const std::vector<LoweredGate>& in, Frames* F, std::vector<RGate>* out) {
+// `scaled`: rotations may leave real scales in the frames (complex128);
+// `lim`: the global factor's scale is flushed once it leaves 2^+-lim.
+void rewrite(const std::vector<LoweredGate>& in, Frames* F, bool scaled, double lim,
+             std::vector<RGate>* out) {
   for (const auto& g : in) {
     if (g.nt == 0) continue;
     const bool diag = is_diagonal(g);
@@ -211,15 +266,22 @@ void rewrite(const std::vector<LoweredGate>& in, Frames* F, std::vector<RGate>* 
       cplx W[4] = {g.m[0], g.m[1] * rq, g.m[2], g.m[3] * rq};
       RGate x;
       x.g = g;
-      if (factor_rotation(W, &x.rot)) {
+      if (factor_rotation(W, scaled, &x.rot)) {
         x.kind = RK_ROT;
-        F->G *= x.rot.a0;
-        F->r[q] = x.rot.a1 / x.rot.a0;
+        F->G *= x.rot.g0;
+        F->r[q] = x.rot.g1 / x.rot.g0;
       } else {
         for (int k = 0; k < 4; ++k) x.g.m[k] = W[k];
         F->r[q] = 1.0;
       }
       out->push_back(x);
+      if (std::fabs(std::log2(std::abs(F->G))) > lim) {
+        // bring the stored amplitudes' scale back (one multiply of the state)
+        Frames sc;
+        sc.G = std::abs(F->G);
+        out->push_back(flush_gate(&sc));
+        F->G /= std::abs(F->G);
+      }
       continue;
     }
     if (diag) {  // controlled or two-qubit diagonal: commutes with the pending diagonal
@@ -272,7 +334,7 @@ struct SlotGate {
 
 int coef_count(const SlotGate& sg) {
   const RGate& r = *sg.rg;
-  if (r.kind == RK_ROT) return 2;
+  if (r.kind == RK_ROT) return 4;  // a pair, aligned, after the two reserved entries
   if (r.kind == RK_FLUSH) return 1 + int(r.flq.size());
   if (sg.diag) return 4;
   return r.g.nt == 1 ? 4 : 16;
@@ -400,8 +462,12 @@ void emit_rot(const SlotGate& sg, const Layout& L, Emitter& E) {
   const Rot& r = sg.rg->rot;
   op.kind = OP1_ROT;
   op.code = uint8_t((r.has_z ? kc_zy : kc_y) + op.ja);
-  E.push(cplx(r.ty, r.sy));
-  if (r.has_z) E.push(cplx(r.tz, r.sz));
+  op.form = uint32_t(r.form);
+  // coefficient pairs start at even indices >= 2 (pair 0 marks "none")
+  while (E.P->ncoef < 2 || (E.P->ncoef & 1)) E.push(0.0);
+  op.coef = uint16_t(E.P->ncoef);
+  E.push(cplx(r.t, r.s));
+  E.push(r.has_z ? cplx(r.tz, r.sz) : cplx(0.0, 0.0));
   E.add(op);
 }
 
@@ -488,7 +554,7 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
     return true;
   };
   while (left > 0) {
-    uint32_t mask = 0, zmask = 0, cidx[4] = {0, 0, 0, 0};
+    uint32_t mask = 0, zmask = 0, pair[4] = {0, 0, 0, 0}, form[4] = {0, 0, 0, 0};
     const uint32_t first_other = uint32_t(P->nothers);
     uint32_t num_other = 0;
     for (int b = 0; b < n; ++b) {
@@ -501,7 +567,8 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
       if (!first) continue;
       mask |= 1u << x.ja;
       if (x.code < kc_y) zmask |= 1u << x.ja;
-      cidx[x.ja] = x.coef;
+      pair[x.ja] = x.coef / 2u;
+      form[x.ja] = x.form;
       state[b] = 2;
       --left;
     }
@@ -516,7 +583,7 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
         grew = true;
       }
     }
-    P->rounds[P->nrounds++] = round_pack(mask, zmask, first_other, num_other, cidx);
+    P->rounds[P->nrounds++] = round_pack(zmask, first_other, num_other, pair, form);
     for (int b = 0; b < n; ++b)
       if (state[b] == 2) state[b] = 1;
   }
@@ -640,10 +707,10 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
   if (int(fr->r.size()) != n) fr->reset(n);
   std::vector<RGate> rg;
   rg.reserve(gates.size() + 2);
-  rewrite(gates, fr, &rg);
-  // keep the carried scale within a few dozen binary orders (it moves only
-  // when non-unitary diagonal gates are absorbed)
+  // keep the carried scale within a few dozen binary orders (it moves with
+  // the scaled rotation forms and non-unitary diagonal gates)
   const double lim = dtype == HS_DTYPE_C64 ? 24.0 : 48.0;
+  rewrite(gates, fr, dtype == HS_DTYPE_C128, lim, &rg);
   if (flush) {
     if (!fr->identity()) rg.push_back(flush_gate(fr));
   } else if (std::fabs(std::log2(std::abs(fr->G))) > lim) {
@@ -652,11 +719,11 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
     rg.push_back(flush_gate(&scale));
     fr->G /= std::abs(fr->G);
   }
-  // two tile buffers must fit in shared memory: 2^11 complex128 / 2^12 complex64
+  // one tile buffer per CTA: up to 2^12 amplitudes (64 KiB of complex128)
   const int max_tile = std::min(n, max_tile_bits(dtype));
   const int rbits = k1_reg_bits(dtype);
   // automatic size: complex128 tiles of 2^10 (CTAs of 64 threads x 16
-  // amplitudes, six per SM), complex64 tiles of 2^12
+  // amplitudes, ten per SM), complex64 tiles of 2^12
   const int auto_m = dtype == HS_DTYPE_C128 ? 10 : max_tile;
   const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : auto_m);
   // keep the lowest slots in the tile so that global accesses come in

@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <stdexcept>
 #include <algorithm>
 #include <vector>
 
@@ -95,7 +96,9 @@ void run_op(std::vector<C>& v, int R, const PartProgram& P, const DevOp& op, con
   if (code < kc_d1) {
     const bool z = code < kc_y;
     const int J = code % 4;
-    const double ty = c[0].x, sy = c[0].y, tz = z ? c[1].x : 0.0, sz = z ? c[1].y : 0.0;
+    // phase shears on B, then the real shears of form op.form
+    const double t = c[0].x, s = c[0].y, tz = z ? c[1].x : 0.0, sz = z ? c[1].y : 0.0;
+    const bool first = !(op.form & 2u), third = !(op.form & 1u);
     pairs(J, [&](int e0, int e1) {
       double ax = v[e0].real(), ay = v[e0].imag(), bx = v[e1].real(), by = v[e1].imag();
       if (z) {
@@ -103,12 +106,16 @@ void run_op(std::vector<C>& v, int R, const PartProgram& P, const DevOp& op, con
         by = std::fma(sz, bx, by);
         bx = std::fma(-tz, by, bx);
       }
-      ax = std::fma(-ty, bx, ax);
-      bx = std::fma(sy, ax, bx);
-      ax = std::fma(-ty, bx, ax);
-      ay = std::fma(-ty, by, ay);
-      by = std::fma(sy, ay, by);
-      ay = std::fma(-ty, by, ay);
+      if (first) {
+        ax = std::fma(t, bx, ax);
+        ay = std::fma(t, by, ay);
+      }
+      bx = std::fma(s, ax, bx);
+      by = std::fma(s, ay, by);
+      if (third) {
+        ax = std::fma(t, bx, ax);
+        ay = std::fma(t, by, ay);
+      }
       v[e0] = C(ax, ay);
       v[e1] = C(bx, by);
     });
@@ -246,16 +253,19 @@ void run_program(const PartProgram& P, int ab, std::vector<C>& sv) {
         uint32_t dsign = 0;
         for (int r = G.first_round; r < G.first_round + G.num_rounds; ++r) {
           const uint64_t rw = P.rounds[r];
-          const uint32_t mask = uint32_t(rw) & 15u, zmask = (uint32_t(rw) >> 4) & 15u;
+          const uint32_t zmask = uint32_t(rw) & 15u;
           for (int j = 0; j < R; ++j) {
-            if (!((mask >> j) & 1)) continue;
+            const uint32_t sw = uint32_t(rw >> (20 + 11 * j)) & 2047u;
+            if (!(sw & 511u)) continue;
             DevOp rop;
             std::memset(&rop, 0, sizeof(rop));
             rop.code = uint8_t((((zmask >> j) & 1) ? kc_zy : kc_y) + j);
-            const uint32_t ci = uint32_t(rw >> (24 + 10 * j)) & 1023u;
+            rop.form = sw >> 9;
+            const uint32_t ci = (sw & 511u) * 2u;
+            if (ci + 2 > uint32_t(P.ncoef)) throw std::runtime_error("rotation coefficients out of range");
             run_op(v, R, P, rop, P.coef + ci, thr, gbase, dsign, ab);
           }
-          const int k0 = int(rw >> 16) & 255, k1 = k0 + (int(rw >> 8) & 255);
+          const int k0 = int(rw >> 12) & 255, k1 = k0 + (int(rw >> 4) & 255);
           for (int k = k0; k < k1; ++k) {
             const DevOp& op = P.ops[P.others[k]];
             run_op(v, R, P, op, P.coef + op.coef, thr, gbase, dsign, ab);
@@ -292,7 +302,8 @@ const char* emu_last_error() { return g_err; }
 // `amps` (2^n interleaved complex128, in/out).  dtype HS_DTYPE_C64 rounds the
 // amplitudes to complex64 as the kernel would.  stats: {passes, groups, ops,
 // rotation ops, max tile bits, rounds, shared-memory wavefronts of the group
-// loads of one tile (summed over programs), the conflict-free count}.
+// loads of one tile (summed over programs), the conflict-free count, rotation
+// ops in a two-shear form}.
 int emu_parts_run(int n, int dtype, const hs_gate* gates, const int32_t* offs, int nparts,
                   int rbits, int tile_hint, int per_part, double* amps, int32_t* stats) {
   g_rbits = rbits;
@@ -302,7 +313,7 @@ int emu_parts_run(int n, int dtype, const hs_gate* gates, const int32_t* offs, i
   for (int q = 0; q < n; ++q) q2s[q] = q;
   Frames fr;
   fr.reset(n);
-  int32_t st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int32_t st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   wave_total = wave_ideal = 0;
   for (int p = 0; p < nparts; ++p) {
     std::vector<LoweredGate> lg(offs[p + 1] - offs[p]);
@@ -316,11 +327,19 @@ int emu_parts_run(int n, int dtype, const hs_gate* gates, const int32_t* offs, i
     if (rc != HS_OK) return rc;
     for (const auto& P : progs) {
       if (P.ngroups < 1 || P.nops < 1) continue;
-      run_program(P, int(amp_bytes(dtype)), sv);
+      try {
+        run_program(P, int(amp_bytes(dtype)), sv);
+      } catch (const std::exception& e) {
+        std::snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return HS_E_INVALID;
+      }
       st[0] += 1;
       st[1] += P.ngroups;
       st[2] += P.nops;
-      for (int i = 0; i < P.nops; ++i) st[3] += P.ops[i].kind == OP1_ROT;
+      for (int i = 0; i < P.nops; ++i) {
+        st[3] += P.ops[i].kind == OP1_ROT;
+        st[8] += P.ops[i].kind == OP1_ROT && P.ops[i].form != 0;
+      }
       st[4] = std::max(st[4], P.m);
       st[5] += P.nrounds;
     }

@@ -43,13 +43,13 @@ def emu(tmp_path_factory):
             a[0] = 1
         else:
             a[:] = init
-        st = np.zeros(8, np.int32)
+        st = np.zeros(9, np.int32)
         rc = lib.emu_parts_run(n, dtype, rec.ctypes.data, offs.ctypes.data, len(offs) - 1, rbits,
                                hint, int(per_part), a.ctypes.data, st.ctypes.data)
         if rc:
             raise RuntimeError(lib.emu_last_error().decode())
         return a, dict(zip(["passes", "groups", "ops", "rotations", "tile_bits", "rounds",
-                            "wavefronts", "wavefronts_ideal"], st.tolist()))
+                            "wavefronts", "wavefronts_ideal", "two_shear"], st.tolist()))
     return run
 
 
@@ -137,3 +137,21 @@ def test_group_loads_are_conflict_free(emu, dtype):
     rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
     _, st = emu(16, rec, offs, dtype=dtype)
     assert st["wavefronts"] == st["wavefronts_ideal"]
+
+
+def test_two_shear_forms_and_scaled_frames(emu, port):
+    """Complex128 programs write most rotations as two shears plus a real
+    scale carried in the frames (complex64 keeps the exact three-shear form);
+    a long circuit, whose frames carry those scales across many parts and
+    calls of the global renormalisation, still matches the oracle."""
+    n = 12
+    gates = circuits.random_u3_cz(n, 60, 21)
+    parts = partition.partition_dfs(gates, 7)
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    got, st = emu(n, rec, offs)
+    assert st["two_shear"] > 0.6 * st["rotations"]
+    assert np.abs(got - want).max() <= 1e-12
+    got64, st64 = emu(n, rec, offs, dtype=1)
+    assert st64["two_shear"] == 0
+    assert np.abs(got64 - want).max() <= 1e-5

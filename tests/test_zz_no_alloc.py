@@ -43,3 +43,34 @@ def test_noalloc_norm_matches_allocating_norm(n, dtype):
 def test_noalloc_rejects_null():
     out = ctypes.c_double()
     assert abi.lib().hs_norm2_noalloc(None, ctypes.byref(out), None) == abi.HS_E_INVALID
+
+
+def test_noalloc_on_a_user_stream():
+    """The stream argument: a stream the caller created (not the legacy default
+    stream), after work queued on that stream wrote the state."""
+    import torch
+
+    n = 18
+    st = abi.State(n, abi.C128)
+    st.run_part(circuits.random_layered(n, 3, 5))
+    want = st.norm2()
+    s = torch.cuda.Stream(device=0)
+    out = ctypes.c_double()
+    for _ in range(3):
+        abi.check(abi.lib().hs_norm2_noalloc(st.h, ctypes.byref(out), ctypes.c_void_p(s.cuda_stream)))
+        assert abs(out.value - want) <= TOL * max(1.0, want)
+
+
+@pytest.mark.skipif(abi.device_count() < 2, reason="needs a second GPU")
+def test_noalloc_on_a_second_device():
+    """The per-device address cache: a state on device 1 after one on device 0."""
+    out = ctypes.c_double()
+    for dev in (0, 1):
+        abi.set_device(dev)
+        st = abi.State(12, abi.C128)
+        st.run_part(circuits.random_layered(12, 2, dev))
+        want = st.norm2()
+        abi.check(abi.lib().hs_norm2_noalloc(st.h, ctypes.byref(out), None))
+        assert abs(out.value - want) <= TOL * max(1.0, want)
+        del st
+    abi.set_device(0)
