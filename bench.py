@@ -4,8 +4,9 @@ Workload (seeded synthetic stand-in for the reference's QASMBench-style
 circuits): 40 layers of U3 with uniform angles on every qubit followed by CZ
 on a random matching (33 is odd: one qubit idles per layer), 1960 gates,
 state |0...0>, acyclic parts of <= k qubits from hisvsim_b200.partition
-(consecutive runs of a DFS topological order by default; --partitioner
-acyclic selects the greedy acyclic partitioner).
+(grown from the DAG's ready frontier by default, the fewest parts;
+--partitioner dfs / acyclic select DFS-order runs or the greedy acyclic
+partitioner).
 
 A step simulates the whole circuit once.  `value` is the plain complex128
 form's throughput in amplitude updates per second (sum over gates of 2^n,
@@ -46,9 +47,10 @@ def parse():
     ap.add_argument("--qubits", type=int, default=33)
     ap.add_argument("--layers", type=int, default=40)
     ap.add_argument("--part-qubits", type=int, default=9)
-    ap.add_argument("--partitioner", default="dfs", choices=["dfs", "acyclic"],
-                    help="acyclic parts from consecutive runs of a DFS topological order "
-                         "(default) or the greedy acyclic partitioner")
+    ap.add_argument("--partitioner", default="frontier", choices=["frontier", "dfs", "acyclic"],
+                    help="acyclic parts grown from the DAG's ready frontier (default, fewest "
+                         "parts), consecutive runs of a DFS topological order, or the greedy "
+                         "acyclic partitioner")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-qubits", type=int, default=26, help="size of the CPU sample")
     ap.add_argument("--cpu-layers", type=int, default=8)
@@ -166,7 +168,8 @@ class ClockSampler:
 def partitioner(args):
     from hisvsim_b200 import partition
 
-    return partition.partition_dfs if args.partitioner == "dfs" else partition.partition_acyclic
+    return {"frontier": partition.partition_frontier, "dfs": partition.partition_dfs,
+            "acyclic": partition.partition_acyclic}[args.partitioner]
 
 
 def workload(n, layers, seed, k, split=None):
@@ -388,18 +391,24 @@ def learned_form(args, abi, pg, device):
             res[k] = learned.measure(st, gates, partition.partition_acyclic(gates, k), reps=1,
                                      warmup=0)
         # the method without the network: the same DP with a trivial cost
-        # (fewest parts), and DFS-order parts at every size (best measured)
+        # (fewest parts), DFS-order and frontier parts at every size (best measured)
         fewest = learned.propose_fewest(gates, n)
         t_fewest = learned.measure(st, gates, fewest["parts"], reps=1, warmup=0)
         t_dfs = {k: learned.measure(st, gates, partition.partition_dfs(gates, k), reps=1, warmup=0)
                  for k in (8, 9, 10, 11, 12)}
+        t_front = {k: learned.measure(st, gates, partition.partition_frontier(gates, k), reps=1,
+                                      warmup=0)
+                   for k in (8, 9, 10, 11, 12)}
     st.close()
     model.close()
     best_k = min(res, key=res.get)
     best_dfs = min(t_dfs, key=t_dfs.get)
+    best_front = min(t_front, key=t_front.get)
     nonlearned = {"dp_fewest_parts_s": t_fewest, "dfs_s": {str(k): v for k, v in t_dfs.items()},
-                  "best_dfs_k": best_dfs, f"acyclic_best_k{best_k}_s": res[best_k]}
-    best_nonlearned = min(t_fewest, t_dfs[best_dfs], res[best_k])
+                  "best_dfs_k": best_dfs,
+                  "frontier_s": {str(k): v for k, v in t_front.items()},
+                  "best_frontier_k": best_front, f"acyclic_best_k{best_k}_s": res[best_k]}
+    best_nonlearned = min(t_fewest, t_dfs[best_dfs], t_front[best_front], res[best_k])
     return {"harvest_parts": int(len(y)), "harvest_qubits": "24..32", "harvest_s": t_h,
             "train_s": t_t, "final_train_mse": float(losses[-1]), "holdout_mean_rel_err": rel,
             "eval": f"random U3+CZ circuit {n} qubits x 40 layers, complex64",
@@ -415,7 +424,7 @@ def learned_form(args, abi, pg, device):
 
 def config1_form(args, abi, peak_gbs, pg, device):
     """Config 1: the 30-qubit QFT (H, controlled phases 2 pi / 2^m on every
-    pair, final swaps) on a seeded random basis state, complex128, DFS-order
+    pair, final swaps) on a seeded random basis state, complex128, frontier
     parts of <= 7 qubits: circuit time, passes and the K1 pass roofline.  And
     the choice the plain path makes for parts on high qubits: a part whose
     qubits are the top ones runs on strided tiles in one pass; the
@@ -428,7 +437,7 @@ def config1_form(args, abi, peak_gbs, pg, device):
 
     n = args.config1_qubits
     gates, x = circuits.qft(n, args.seed)
-    parts = partition.partition_dfs(gates, 7)
+    parts = partition.partition_frontier(gates, 7)
     rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
     st = abi.State(n, abi.C128)
 
@@ -469,7 +478,7 @@ def config1_form(args, abi, peak_gbs, pg, device):
     ms_swap = dev_ms(lambda: st.permute_bits(pairs[:5]), reps=4)
     st.close()
     return {"workload": f"QFT {n} qubits on a random basis state, {len(gates)} gates, "
-                        f"{len(parts)} DFS-order parts of <= 7 qubits, complex128",
+                        f"{len(parts)} frontier parts of <= 7 qubits, complex128",
             "circuit_s": t, "passes_per_step": passes, "value": len(gates) * float(1 << n) / t,
             "unit": UNIT,
             "roofline": {"bound": "hbm", "kernel": "k1_part", "avg_launch_ms": k1_ms,

@@ -5,8 +5,9 @@
 // qubits, the 2^k amplitudes of the part's qubits into an inner state vector,
 // applying every gate there and scattering back (execute.hpp:318-470,
 // state_vector.hpp:617-673; the loop nest of loop.hpp:468-962).  Here a tile
-// is the same gather, widened by the lowest slots so that every global access
-// moves whole 32-byte sectors (the GPU form of opt_slots, execute.hpp:184-199).
+// is the same gather, widened by the three lowest slots so that every global
+// access moves whole 128-byte lines of complex128 (the GPU form of opt_slots,
+// execute.hpp:184-199).
 // Each tile is held by one CTA: 2^R amplitudes per thread in registers, where
 // R tile bits are "register bits".  A non-diagonal gate's targets must be
 // register bits; consecutive gates whose targets fit in R bits form a group,
@@ -726,10 +727,12 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
   // amplitudes, ten per SM), complex64 tiles of 2^12
   const int auto_m = dtype == HS_DTYPE_C128 ? 10 : max_tile;
   const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : auto_m);
-  // keep the lowest slots in the tile so that global accesses come in
-  // contiguous runs of at least 64 bytes (complex64 tiles also need slot 0 for
-  // their 16-byte chunks)
-  const int low_min = std::min(n, dtype == HS_DTYPE_C64 ? 3 : 2);
+  // keep the three lowest slots in the tile so that global accesses come in
+  // contiguous runs of at least 8 amplitudes (128 bytes of complex128: whole
+  // L2 lines; with 64-byte runs the other half of each line is fetched as
+  // well and often evicted before its own tile reads it -- 3.7% slower at 33
+  // qubits); complex64 tiles also need slot 0 for their 16-byte chunks
+  const int low_min = std::min(n, 3);
   std::vector<SlotGate> sgs;
   sgs.reserve(rg.size());
   for (const auto& r : rg) {

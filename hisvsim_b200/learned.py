@@ -10,9 +10,11 @@ on itself (``harvest``: ``hs_parts_run_timed`` over seeded random circuits).
 ``propose`` chooses a partition of a circuit:
   * for every part size k, the acyclic partitioner's parts (the method without
     the network: ``partition.partition_acyclic``, the role of the reference's
-    dagP/acyclic part files), scored by the network;
-  * for several topological orders (DFS, and the acyclic partitioner's own
-    order at its best k), a dynamic program over cut points: every contiguous
+    dagP/acyclic part files) and the frontier partitioner's
+    (``partition.partition_frontier``), scored by the network;
+  * for several topological orders (DFS, the acyclic partitioner's own order
+    at its best k, the frontier partition's order at its best k, the listed
+    order), a dynamic program over cut points: every contiguous
     segment of the order with at most ``max_qubits`` qubits is a valid acyclic
     part, the network prices each, and the cheapest segmentation wins.
 The acyclic partitioner is the fallback: without a model, or when no
@@ -171,14 +173,21 @@ def propose(gates: Sequence[Gate], n: int, model: Optional[CostModel], dtype: in
                 "candidates": {}}
     cands = {}
     best_k, best_k_ms = default_k, np.inf
+    best_f, best_f_ms, best_f_parts = default_k, np.inf, None
     for k in ks:
         parts = partition.partition_acyclic(gates, k)
         ms = float(model.predict_ms(abi.part_features(n, gates, parts, dtype), n).sum())
         cands[f"acyclic k={k}"] = (ms, parts)
         if ms < best_k_ms:
             best_k, best_k_ms = k, ms
+        fparts = partition.partition_frontier(gates, k)
+        fms = float(model.predict_ms(abi.part_features(n, gates, fparts, dtype), n).sum())
+        cands[f"frontier k={k}"] = (fms, fparts)
+        if fms < best_f_ms:
+            best_f, best_f_ms, best_f_parts = k, fms, fparts
     orders = {"dfs": partition.dfs_order(gates),
               f"acyclic-order k={best_k}": acyclic_order(gates, best_k),
+              f"frontier-order k={best_f}": [i for p in best_f_parts for i in p],
               "listed": list(range(len(gates)))}
     for name, order in orders.items():
         st, ln, ft = abi.order_segments(n, gates, order, max_qubits, max_len, dtype)
@@ -201,7 +210,8 @@ def propose_fewest(gates: Sequence[Gate], n: int, dtype: int = abi.C64, max_qubi
     1: the fewest parts) over the same orders and segment limits: the method
     without the network, for measuring what the network adds."""
     best = None
-    orders = {"dfs": partition.dfs_order(gates), "listed": list(range(len(gates)))}
+    orders = {"dfs": partition.dfs_order(gates), "listed": list(range(len(gates))),
+              "frontier": [i for p in partition.partition_frontier(gates, max_qubits) for i in p]}
     for name, order in orders.items():
         st, ln, _ = abi.order_segments(n, gates, order, max_qubits, max_len, dtype)
         cuts, total = _dp(st, ln, np.ones(len(st)), len(order))

@@ -125,12 +125,15 @@ def test_learned_proposal_beats_acyclic_partitioner():
     assert t_learned < 0.97 * t_default, (t_learned, t_default)
     assert t_learned < t_best, (t_learned, t_best, best_k)
     # what the network adds beyond the method without it: the same dynamic
-    # program with a trivial cost (fewest parts), and DFS-order parts at the
-    # best part size found by measuring every size
+    # program with a trivial cost (fewest parts), and DFS-order and frontier
+    # parts at the best part size found by measuring every size
     st = abi.State(n, abi.C64)
     t_fewest = learned.measure(st, gates, learned.propose_fewest(gates, n)["parts"], reps=3)
     t_dfs = {k: learned.measure(st, gates, partition.partition_dfs(gates, k), reps=2)
              for k in (8, 9, 10, 11, 12)}
+    t_front = {k: learned.measure(st, gates, partition.partition_frontier(gates, k), reps=2)
+               for k in (8, 9, 10, 11, 12)}
     st.close()
     assert t_learned < t_fewest, (t_learned, t_fewest)
     assert t_learned <= 1.02 * min(t_dfs.values()), (t_learned, t_dfs)
+    assert t_learned <= 1.02 * min(t_front.values()), (t_learned, t_front)

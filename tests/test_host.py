@@ -250,3 +250,18 @@ def test_index_checks_only_in_the_checked_build():
     L = ctypes.CDLL(path)
     missing = [n for n in header_functions() if not hasattr(L, n)]
     assert not missing, missing
+
+
+@pytest.mark.parametrize("k", [3, 6, 9])
+def test_frontier_partition_valid_and_fewer(k):
+    """The frontier partitioner gives valid acyclic parts under the qubit
+    limit, and fewer than the DFS-order runs on layered circuits."""
+    for gates in (circuits.random_u3_cz(16, 12, k), circuits.random_layered(12, 6, k)):
+        parts = partition.partition_frontier(gates, k)
+        assert partition.is_valid_partition(gates, parts)
+        for p in parts:
+            assert len({q for i in p for q in gates[i].qubits}) <= k
+    g = circuits.random_u3_cz(33, 40, 2024)
+    assert len(partition.partition_frontier(g, k)) < 0.9 * len(partition.partition_dfs(g, k))
+    with pytest.raises(ValueError):
+        partition.partition_frontier([Gate("X", (0,), (1, 2))], 2)
