@@ -727,11 +727,11 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
   // amplitudes, ten per SM), complex64 tiles of 2^12
   const int auto_m = dtype == HS_DTYPE_C128 ? 10 : max_tile;
   const int m_target = std::min(max_tile, tile_bits_hint > 0 ? tile_bits_hint : auto_m);
-  // keep the three lowest slots in the tile so that global accesses come in
-  // contiguous runs of at least 8 amplitudes (128 bytes of complex128: whole
-  // L2 lines; with 64-byte runs the other half of each line is fetched as
-  // well and often evicted before its own tile reads it -- 3.7% slower at 33
-  // qubits); complex64 tiles also need slot 0 for their 16-byte chunks
+  // keep the three lowest slots in the tile where they fit, so that global
+  // accesses come in contiguous runs of at least 8 amplitudes (128 bytes of
+  // complex128: whole L2 lines; with 64-byte runs the other half of each
+  // line is fetched as well and often evicted before its own tile reads it
+  // -- 3.7% slower at 33 qubits)
   const int low_min = std::min(n, 3);
   std::vector<SlotGate> sgs;
   sgs.reserve(rg.size());
@@ -752,12 +752,16 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
     }
     sgs.push_back(std::move(s));
   }
-  auto low_union_size = [&](const std::vector<int>& t) {
+  auto low_union_size = [&](const std::vector<int>& t, int lows) {
     int extra = 0;
-    for (int s = 0; s < low_min; ++s)
+    for (int s = 0; s < lows; ++s)
       if (std::find(t.begin(), t.end(), s) == t.end()) ++extra;
     return int(t.size()) + extra;
   };
+  // a chunk only needs the low slots the 16-byte chunk copy requires (slot 0
+  // for complex64); where the targets leave room the tile takes all three:
+  // shorter runs cost less than another pass
+  const int low_need = std::min(n, dtype == HS_DTYPE_C64 ? 1 : 0);
   size_t gi = 0;
   while (gi < sgs.size()) {
     // ---- chunk: gates whose non-diagonal target slots (+ low slots) fit one tile
@@ -772,7 +776,7 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
       const int cc = coef_count(sgs[gend]);
       const int nops_g = sgs[gend].rg->kind == RK_FLUSH ? 1 + int(sgs[gend].rg->flq.size()) : 1;
       const int nfl_g = sgs[gend].rg->kind == RK_FLUSH ? int(sgs[gend].rg->flq.size()) : 0;
-      if (low_union_size(t2) > max_tile || ops + nops_g > kMaxOps || coefs + cc > kMaxCoef ||
+      if (low_union_size(t2, low_need) > max_tile || ops + nops_g > kMaxOps || coefs + cc > kMaxCoef ||
           fls + nfl_g > kMaxFlush)
         break;
       tset = t2;
@@ -784,7 +788,7 @@ int plan_gates(int n, const std::vector<int>& q2s, const std::vector<LoweredGate
     if (gend == gi) return set_error(HS_E_INVALID, "gate does not fit a tile");
     // ---- tile: non-diagonal target slots + lowest slots up to the target size
     std::vector<int> tile = tset;
-    const int m = std::min(max_tile, std::max(m_target, low_union_size(tset)));
+    const int m = std::min(max_tile, std::max(m_target, low_union_size(tset, low_min)));
     for (int s = 0; s < n && int(tile.size()) < m; ++s)
       if (std::find(tile.begin(), tile.end(), s) == tile.end()) tile.push_back(s);
     std::sort(tile.begin(), tile.end());

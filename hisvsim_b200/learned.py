@@ -55,14 +55,18 @@ def _circuit(n: int, layers: int, seed: int) -> List[Gate]:
 
 def sample_parts(gates: Sequence[Gate], rng: np.random.Generator, count: int,
                  max_qubits: int = 13) -> List[List[int]]:
-    """Parts like those the proposer will price: acyclic parts of random k and
-    random contiguous segments of DFS / acyclic orders under random qubit caps."""
+    """Parts like those the proposer will price: acyclic and frontier parts of
+    random k and random contiguous segments of DFS / acyclic / frontier orders
+    under random qubit caps."""
     orders = [partition.dfs_order(gates)]
     orders += [acyclic_order(gates, int(k)) for k in rng.choice(np.arange(4, 13), 2, replace=False)]
+    front = partition.partition_frontier(gates, int(rng.integers(4, 13)))
+    orders.append([i for p in front for i in p])
     qm = [set(g.controls) | set(g.targets) for g in gates]
     out: List[List[int]] = []
     acyc = partition.partition_acyclic(gates, int(rng.integers(4, 13)))
-    out += [list(p) for p in acyc[: count // 4]]
+    out += [list(p) for p in acyc[: count // 8]]
+    out += [list(p) for p in front[: count // 8]]
     while len(out) < count:
         order = orders[int(rng.integers(len(orders)))]
         cap = int(rng.integers(2, max_qubits + 1))

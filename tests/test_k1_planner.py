@@ -155,3 +155,23 @@ def test_two_shear_forms_and_scaled_frames(emu, port):
     got64, st64 = emu(n, rec, offs, dtype=1)
     assert st64["two_shear"] == 0
     assert np.abs(got64 - want).max() <= 1e-5
+
+
+def test_targets_filling_the_tile_leave_out_low_slots(emu, port):
+    """A part whose non-diagonal targets fill the largest tile (12 qubits, none
+    of them low) runs as one pass without the low slots (shorter contiguous
+    runs rather than a second pass); complex64 keeps slot 0 (its 16-byte
+    chunks), so there it takes two."""
+    rng = np.random.default_rng(5)
+    n = 16
+    qs = list(range(3, 15))
+    gates = [Gate("U3", (q,), params=tuple(rng.uniform(0, 2 * np.pi, 3))) for q in qs]
+    gates += [Gate("Z", (qs[i + 1],), (qs[i],)) for i in range(0, 12, 2)]
+    rec, offs = part_offsets([gates])
+    want = port.run(n, to_records(gates))
+    got, st = emu(n, rec, offs)
+    assert st["passes"] == 1 and st["tile_bits"] == 12
+    assert np.abs(got - want).max() <= 1e-12
+    got64, st64 = emu(n, rec, offs, dtype=1)
+    assert st64["passes"] == 2
+    assert np.abs(got64 - want).max() <= 1e-5
