@@ -916,7 +916,13 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
     const int c_begin = half * per;
     const int c_end = c_begin + per < N ? c_begin + per : N;
     float* stg = stage + (warp - 8) * kBulkStageFloats;
-    auto sidx = [](int p, int c) { return p * 32 + ((c ^ ((p & 7) << 1)) << 1); };
+    // column c of part row p sits at word 2 (c ^ f(p)), f(p) = 2 (p mod 8) +
+    // (p div 8): the 16 rows x (re, im) of one column hit 32 distinct banks;
+    // a column pair (c, c + 1), c even, stays one 16-byte slot (spair), in
+    // reversed order for rows p >= 8 (odd f)
+    auto fsw = [](int p) { return ((p & 7) << 1) | ((p >> 3) & 1); };
+    auto sidx = [&](int p, int c) { return p * 32 + ((c ^ fsw(p)) << 1); };
+    auto spair = [&](int p, int c) { return p * 32 + (((c ^ fsw(p)) & ~1) << 1); };
     const uint64_t* gpq = gp + quad * 16;
     for (uint64_t i = 0; i < cnt && !*abort_flag; ++i) {
       const int b = int(i & 1);
@@ -937,7 +943,8 @@ __global__ void __launch_bounds__(kBulkThreads, 1)
 #pragma unroll
           for (int s4 = 0; s4 < 4; ++s4) {
             const int p = (lane >> 3) + 4 * s4, c = 2 * (lane & 7);
-            const float4 v = *reinterpret_cast<const float4*>(stg + sidx(p, c));
+            float4 v = *reinterpret_cast<const float4*>(stg + spair(p, c));
+            if (s4 >= 2) v = make_float4(v.z, v.w, v.x, v.y);  // p >= 8
             if (HS_IN_BOUNDS(uint64_t(tb - sv) + gpq[p] + gn[c0 + c] + 2 <= (1ull << P.n), kBoundsK4))
               __stcs(reinterpret_cast<float4*>(tb + gpq[p] + gn[c0 + c]), v);
           }
@@ -1222,7 +1229,13 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
     const int c_begin = half * per;
     const int c_end = c_begin + per < N ? c_begin + per : N;
     float* stg = stage + (warp - 8) * kBulkStageFloats;
-    auto sidx = [](int p, int c) { return p * 32 + ((c ^ ((p & 7) << 1)) << 1); };
+    // column c of part row p sits at word 2 (c ^ f(p)), f(p) = 2 (p mod 8) +
+    // (p div 8): the 16 rows x (re, im) of one column hit 32 distinct banks;
+    // a column pair (c, c + 1), c even, stays one 16-byte slot (spair), in
+    // reversed order for rows p >= 8 (odd f)
+    auto fsw = [](int p) { return ((p & 7) << 1) | ((p >> 3) & 1); };
+    auto sidx = [&](int p, int c) { return p * 32 + ((c ^ fsw(p)) << 1); };
+    auto spair = [&](int p, int c) { return p * 32 + (((c ^ fsw(p)) & ~1) << 1); };
     auto drain = [&](int s2, uint64_t i) -> bool {
       const int b = int(i & 1);
       if (!tc::mbar_wait(&mdone[2 * s2 + b], ph(i), kWaitLimit)) {
@@ -1253,7 +1266,8 @@ __global__ void __launch_bounds__(kBulk2Threads, 1)
           if (pairs) {
             p = (lane >> 3) + 4 * s4;
             c = 2 * (lane & 7);
-            v = *reinterpret_cast<const float4*>(stg + sidx(p, c));
+            v = *reinterpret_cast<const float4*>(stg + spair(p, c));
+            if (s4 >= 2) v = make_float4(v.z, v.w, v.x, v.y);  // p >= 8
           } else {
             p = 2 * ((lane >> 4) + 2 * s4);
             c = lane & 15;
