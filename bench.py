@@ -204,10 +204,14 @@ def cpu_sample(args, threads, full_size=False):
     t = time.perf_counter()
     ref.run(n, rec, offs, mode=1, opt_slots=1, threads=threads)
     t_part = time.perf_counter() - t
-    out = {"value": upd / t_gate, "unit": UNIT, "cores": threads, "kind": "reference",
+    # the baseline is the faster of the reference's two live paths
+    faster = "parts" if t_part < t_gate else "per_gate"
+    out = {"value": upd / min(t_gate, t_part), "unit": UNIT, "cores": threads,
+           "kind": "reference",
            "sample": f"{n} qubits x {layers} layers of the same circuit family ({len(gates)} gates, "
-                     f"{len(parts)} parts of <= {args.part_qubits} qubits), all host threads",
-           "seconds": t_gate,
+                     f"{len(parts)} parts of <= {args.part_qubits} qubits), all host threads; "
+                     f"value = the faster of the two live paths ({faster})",
+           "seconds": min(t_gate, t_part), "path": faster,
            "per_gate": {"entry": "BoundGate::apply (state_vector.hpp:1349)", "seconds": t_gate,
                         "value": upd / t_gate},
            "parts": {"entry": "gather_and_execute_on_multi, opt_slots=1 (execute.hpp:318-470)",
@@ -230,14 +234,17 @@ def run_reference_arm(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     threads = os.cpu_count() or 1
-    vals, parts_vals = [], []
+    gate_vals, parts_vals = [], []
     r = None
     for i in range(args.warmup + args.steps):
         r = cpu_sample(args, threads)
         if i >= args.warmup:
-            vals.append(r["value"])
+            gate_vals.append(r["per_gate"]["value"])
             parts_vals.append(r["parts"]["value"])
-    v = statistics.mean(vals)
+    # the faster of the reference's two live paths, averaged over the steps
+    g_mean, p_mean = statistics.mean(gate_vals), statistics.mean(parts_vals)
+    v = max(g_mean, p_mean)
+    faster = "gather_and_execute_on_multi" if p_mean > g_mean else "BoundGate::apply"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -247,10 +254,11 @@ def run_reference_arm(args):
                                    f"and ~2 h of CPU per step)",
                        "parallelism": "replicas"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": r["sample"] + "; value = per-gate BoundGate::apply, "
-                                       "the faster of the reference's two live paths"},
-            "parts_path": {"entry": r["parts"]["entry"], "value": statistics.mean(parts_vals),
-                           "unit": UNIT},
+                             "sample": r["sample"].split("; value")[0] +
+                                       f"; value = {faster}, the faster of the reference's "
+                                       "two live paths"},
+            "per_gate_path": {"entry": r["per_gate"]["entry"], "value": g_mean, "unit": UNIT},
+            "parts_path": {"entry": r["parts"]["entry"], "value": p_mean, "unit": UNIT},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

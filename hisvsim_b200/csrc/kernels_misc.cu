@@ -327,12 +327,6 @@ struct TilePerm {
   int32_t m, np;
   uint64_t ntiles;
   uint8_t pa[8], pb[8];  // tile-bit positions of each pair
-  // shared-memory swizzle: element j sits at j ^ XOR_i (bit sh[i] of j) << sl[i]
-  // for the pairs that exchange a bank bit (sl < 3 for 16-byte, < 4 for
-  // 8-byte elements) with a higher bit sh, so the lanes of a read at the
-  // exchanged position still hit distinct banks
-  int32_t nsw;
-  uint8_t sl[8], sh[8];
 };
 
 __device__ __forceinline__ uint64_t dep_runs(uint64_t x, const Runs& r) {
@@ -363,16 +357,11 @@ __global__ void __launch_bounds__(kK2Threads) k2_tile(V* __restrict__ sv, const 
   const uint64_t gt = dep_runs(uint64_t(t), P.tile);
   const uint32_t sb = uint32_t(__cvta_generic_to_shared(bufs));
   const uint64_t size = P.ntiles << P.m;  // amplitudes of the state (bounds checks)
-  auto swz = [&](uint32_t j) {
-    uint32_t x = j;
-    for (int i = 0; i < P.nsw; ++i) x ^= ((j >> P.sh[i]) & 1u) << P.sl[i];
-    return x;
-  };
   auto issue = [&](uint64_t tile, int b) {
     if (!active) return;
     const uint64_t gb = dep_runs(tile, P.outer) + gt;
     for (int k = 0; k < per; ++k) {
-      const uint32_t j = swz(uint32_t(t + k * kK2Threads));
+      const uint32_t j = uint32_t(t + k * kK2Threads);
       if (HS_IN_BOUNDS(gb + gk[k] < size && j < uint32_t(T), kBoundsK2))
         cp_async_el<sizeof(V)>(sb + uint32_t((b * T + j) * sizeof(V)), sv + gb + gk[k]);
     }
@@ -395,7 +384,6 @@ __global__ void __launch_bounds__(kK2Threads) k2_tile(V* __restrict__ sv, const 
           const uint32_t d = ((j >> P.pa[i]) ^ (j >> P.pb[i])) & 1u;
           j ^= d * ((1u << P.pa[i]) | (1u << P.pb[i]));
         }
-        j = swz(j);
         if (HS_IN_BOUNDS(gb + gk[k] < size && j < uint32_t(T), kBoundsK2))
           __stcs(sv + gb + gk[k], cur[j]);
       }
@@ -441,18 +429,9 @@ int launch_tile_perm(V* amp, int n, const int32_t* pairs, int np, int max_bits, 
   runs_from(outer, &P.outer);
   if (P.tile.n > kMaxRuns || P.outer.n > kMaxRuns)
     return set_error(HS_E_UNSUPPORTED, "bit-swap tile has too many runs");
-  // bank bits: the element's slot within a 128-byte row
-  const int bank_bits = sizeof(V) == 16 ? 3 : 4;
-  P.nsw = 0;
   for (int i = 0; i < np; ++i) {
     P.pa[i] = uint8_t(std::find(tile.begin(), tile.end(), pairs[2 * i]) - tile.begin());
     P.pb[i] = uint8_t(std::find(tile.begin(), tile.end(), pairs[2 * i + 1]) - tile.begin());
-    const int lo = std::min(P.pa[i], P.pb[i]), hi = std::max(P.pa[i], P.pb[i]);
-    if (lo < bank_bits && hi >= bank_bits) {
-      P.sl[P.nsw] = uint8_t(lo);
-      P.sh[P.nsw] = uint8_t(hi);
-      ++P.nsw;
-    }
   }
   const int T = 1 << P.m;
   const int per = T > kK2Threads ? T / kK2Threads : 1;
