@@ -63,6 +63,11 @@ SIGNATURES = {
     "hs_state_convert": [_vp, _vp, _vp],
     "hs_gate_apply": [_vp, _vp, _vp],
     "hs_part_run": [_vp, _vp, _i, _vp],
+    "hs_frames_create": [_i, ctypes.POINTER(_vp)],
+    "hs_frames_destroy": [_vp],
+    "hs_frames_pending": [_vp, ctypes.POINTER(_i)],
+    "hs_part_run_carry": [_vp, _vp, _vp, _i, _vp],
+    "hs_frames_flush": [_vp, _vp, _vp],
     "hs_parts_run": [_vp, _vp, _vp, _i, _vp],
     "hs_set_tile_qubits": [_i],
     "hs_set_k1_reg_bits": [_i],
@@ -240,6 +245,14 @@ class State:
         rec = _records(gates)
         check(lib().hs_part_run(self.h, _ptr(rec), len(rec), stream))
 
+    def run_part_carry(self, frames: "Frames", gates, stream=None):
+        """hs_part_run_carry: the part's pending factors stay in `frames`."""
+        rec = _records(gates)
+        check(lib().hs_part_run_carry(self.h, frames.h, _ptr(rec), len(rec), stream))
+
+    def flush(self, frames: "Frames", stream=None):
+        check(lib().hs_frames_flush(self.h, frames.h, stream))
+
     def run_parts(self, records: np.ndarray, offsets: np.ndarray, stream=None):
         records = _records(records)
         offsets = np.ascontiguousarray(offsets, dtype=np.int32)
@@ -388,6 +401,31 @@ def set_device(d: int):
 
 def synchronize():
     check(lib().hs_device_synchronize())
+
+
+class Frames:
+    """Pending per-qubit factors carried between part calls (hs_frames)."""
+
+    def __init__(self, n: int):
+        self.h = _vp()
+        check(lib().hs_frames_create(n, ctypes.byref(self.h)))
+
+    @property
+    def pending(self) -> bool:
+        p = _i()
+        check(lib().hs_frames_pending(self.h, ctypes.byref(p)))
+        return bool(p.value)
+
+    def close(self):
+        if self.h:
+            lib().hs_frames_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Event:

@@ -346,6 +346,62 @@ int hs_part_run(hs_state* st, const hs_gate* gates, int num_gates, void* stream)
   return run_lowered(st, lg, num_gates, S(stream));
 }
 
+int hs_frames_create(int num_qubits, hs_frames** out) {
+  if (!out) return set_error(HS_E_INVALID, "null output pointer");
+  if (num_qubits < 1 || num_qubits > 63) return set_error(HS_E_INVALID, "bad qubit count %d", num_qubits);
+  hs_frames* f = new (std::nothrow) hs_frames;
+  if (!f) return set_error(HS_E_NOMEM, "frames");
+  f->n = num_qubits;
+  f->fr.reset(num_qubits);
+  *out = f;
+  return HS_OK;
+}
+
+int hs_frames_destroy(hs_frames* fr) {
+  delete fr;
+  return HS_OK;
+}
+
+int hs_frames_pending(const hs_frames* fr, int* pending) {
+  if (!fr || !pending) return set_error(HS_E_INVALID, "null argument");
+  *pending = fr->fr.identity() ? 0 : 1;
+  return HS_OK;
+}
+
+int hs_part_run_carry(hs_state* st, hs_frames* fr, const hs_gate* gates, int num_gates,
+                      void* stream) {
+  HS_TRY(check_state(st));
+  if (!fr || fr->n != st->n) return set_error(HS_E_INVALID, "frames missing or of another size");
+  if (num_gates < 0 || (num_gates > 0 && !gates)) return set_error(HS_E_INVALID, "bad gate list");
+  if (num_gates == 0) return HS_OK;
+  std::vector<LoweredGate> lg;
+  HS_TRY(lower_all(st, gates, num_gates, &lg));
+  std::vector<PartProgram> progs;
+  HS_TRY(plan_gates(st->n, st->q2s, lg, &fr->fr, false, g_tile_hint.load(), st->dtype, &progs));
+  TimedRegion tr(S(stream));
+  for (const auto& pr : progs) {
+    HS_TRY(launch_part(st->amp, st->dtype, pr, S(stream)));
+    count_pass(pr.nops);
+    g_param_bytes += (long long)sizeof(PartProgram);
+  }
+  return HS_OK;
+}
+
+int hs_frames_flush(hs_state* st, hs_frames* fr, void* stream) {
+  HS_TRY(check_state(st));
+  if (!fr || fr->n != st->n) return set_error(HS_E_INVALID, "frames missing or of another size");
+  if (fr->fr.identity()) return HS_OK;
+  std::vector<PartProgram> progs;
+  HS_TRY(plan_gates(st->n, st->q2s, {}, &fr->fr, true, g_tile_hint.load(), st->dtype, &progs));
+  TimedRegion tr(S(stream));
+  for (const auto& pr : progs) {
+    HS_TRY(launch_part(st->amp, st->dtype, pr, S(stream)));
+    count_pass(pr.nops);
+    g_param_bytes += (long long)sizeof(PartProgram);
+  }
+  return HS_OK;
+}
+
 int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
                  int num_parts, void* stream) {
   HS_TRY(check_state(st));

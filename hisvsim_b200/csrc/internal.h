@@ -396,6 +396,12 @@ int launch_mlp_adam(float* params, const float* grad, float* m, float* v, int P,
 
 }  // namespace hisv
 
+// pending factors carried between hs_part_run_carry calls
+struct hs_frames {
+  int n = 0;
+  hisv::Frames fr;
+};
+
 struct hs_state {
   int n = 0;
   int dtype = HS_DTYPE_C128;

@@ -156,16 +156,29 @@ std::mt19937_64 g_seed_gen(std::random_device{}());
 
 struct SV {  // StateVector
   hs_state* st = nullptr;
+  // factors that gather_and_execute_on / BoundGate.apply leave pending
+  // (hs_part_run_carry); every method that reads or writes the amplitudes
+  // applies them first (settle), so the object behaves as the reference's
+  // StateVector after each call
+  hs_frames* fr = nullptr;
   int n = 0;
   SV(int num_qubits, int numa) {
     (void)numa;  // allocation policy of host memory; the state lives in HBM
     py::gil_scoped_release nogil;
     check(hs_state_create(num_qubits, HS_DTYPE_C128, &st));
     n = num_qubits;
+    const int rc = hs_frames_create(num_qubits, &fr);
+    if (rc != HS_OK) {
+      hs_state_destroy(st);
+      st = nullptr;
+      check(rc);
+    }
   }
   ~SV() {
+    if (fr) hs_frames_destroy(fr);
     if (st) hs_state_destroy(st);
   }
+  void settle() { check(hs_frames_flush(st, fr, nullptr)); }
   std::vector<int> qubits() const {
     std::vector<int> q(n);
     for (int i = 0; i < n; ++i) q[i] = i;
@@ -175,6 +188,7 @@ struct SV {  // StateVector
     py::array_t<std::complex<double>> out(size_t(1) << n);
     {
       py::gil_scoped_release nogil;
+      settle();
       check(hs_state_canonicalize(st, nullptr));
     }
     check(hs_state_copy_to_host(st, out.mutable_data(), 0, uint64_t(1) << n, nullptr));
@@ -182,6 +196,7 @@ struct SV {  // StateVector
   }
   void load(py::array_t<std::complex<double>, py::array::c_style | py::array::forcecast> a) {
     if (size_t(a.size()) != (size_t(1) << n)) throw py::value_error("need 2^n amplitudes");
+    settle();  // (the pending factors then reset; the amplitudes are overwritten)
     check(hs_state_set_basis(st, 0, nullptr));
     check(hs_state_copy_from_host(st, a.data(), 0, uint64_t(1) << n, nullptr));
   }
@@ -190,6 +205,7 @@ struct SV {  // StateVector
     std::vector<int32_t> q(qs.begin(), qs.end());
     {
       py::gil_scoped_release nogil;
+      settle();
       check(hs_measure(st, q.data(), int(q.size()), nsamples, g_seed_gen(), out.data()));
     }
     std::vector<std::vector<int>> r(nsamples, std::vector<int>(qs.size()));
@@ -200,6 +216,8 @@ struct SV {  // StateVector
   double max_abs_diff(SV& o) {
     double d = 0;
     py::gil_scoped_release nogil;
+    settle();
+    o.settle();
     check(hs_max_abs_diff(st, o.st, &d));
     return d;
   }
@@ -220,12 +238,14 @@ struct SV {  // StateVector
   double norm() {
     double s = 0;
     py::gil_scoped_release nogil;
+    settle();
     check(hs_norm2(st, &s));
     return s;
   }
   double probability(int q, int v) {
     double p = 0;
     py::gil_scoped_release nogil;
+    settle();
     check(hs_probability(st, q, v, &p));
     return p;
   }
@@ -243,7 +263,7 @@ struct Bound {  // BoundGate (state_vector.hpp:1332-1379)
   }
   void apply(SV& sv) {
     py::gil_scoped_release nogil;
-    check(hs_gate_apply(sv.st, &rec, nullptr));
+    check(hs_part_run_carry(sv.st, sv.fr, &rec, 1, nullptr));
   }
 };
 
@@ -259,7 +279,7 @@ void gather_and_execute_on(SV& sv, std::vector<Bound*> gates) {
   auto t0 = std::chrono::steady_clock::now();
   {
     py::gil_scoped_release nogil;
-    check(hs_part_run(sv.st, recs.data(), int(recs.size()), nullptr));
+    check(hs_part_run_carry(sv.st, sv.fr, recs.data(), int(recs.size()), nullptr));
   }
   g_gather_us += std::chrono::duration_cast<std::chrono::microseconds>(
                      std::chrono::steady_clock::now() - t0).count();
@@ -302,7 +322,8 @@ SV* gather_and_execute_on_mpi(int n, int nlocal, std::vector<std::vector<Bound*>
     py::gil_scoped_release nogil;
     if (p > 0 && !proc.empty())
       check(hs_gather_qubits(sv->st, proc.data(), int(proc.size()), nullptr));
-    check(hs_part_run(sv->st, recs.data(), int(recs.size()), nullptr));
+    // the pending factors belong to qubits: they follow the gather
+    check(hs_part_run_carry(sv->st, sv->fr, recs.data(), int(recs.size()), nullptr));
   }
   return sv.release();
 }

@@ -176,6 +176,27 @@ int hs_parts_run(hs_state* st, const hs_gate* gates, const int32_t* part_offsets
 int hs_parts_run_timed(hs_state* st, const hs_gate* gates, const int32_t* part_offsets,
                        int num_parts, float* part_ms, void* stream);
 
+/* Deferred factors between part calls (no counterpart in the reference).
+ * hs_part_run leaves the stored amplitudes exact after every call, so each
+ * call applies the phase / scale factors its one-qubit rotations leave
+ * pending (one op at the end of the part).  A caller that runs parts one call
+ * at a time (the reference's gather_and_execute_on loop) can keep them
+ * pending instead: hs_part_run_carry applies a part with the pending factors
+ * of `fr` carried in and out, as hs_parts_run does between its parts, and
+ * hs_frames_flush applies whatever is pending (one pass over the state, none
+ * when nothing is).  While factors are pending the true state is the stored
+ * amplitudes times them: flush before any other entry point reads or writes
+ * the state.  The factors belong to qubits, so qubit permutations
+ * (hs_permute_bits, hs_gather_qubits) may come in between. */
+typedef struct hs_frames hs_frames;
+int hs_frames_create(int num_qubits, hs_frames** out);
+int hs_frames_destroy(hs_frames* fr);
+/* *pending = 1 while any factor is pending */
+int hs_frames_pending(const hs_frames* fr, int* pending);
+int hs_part_run_carry(hs_state* st, hs_frames* fr, const hs_gate* gates, int num_gates,
+                      void* stream);
+int hs_frames_flush(hs_state* st, hs_frames* fr, void* stream);
+
 /* Host-only: plan one part (identity slot map) without touching a device and
  * report stats[0..5] = {passes, register groups, ops, dense ops, diagonal
  * ops, tile bits}.  Used by the cost model and by tests of the planner. */
