@@ -265,3 +265,16 @@ def test_frontier_partition_valid_and_fewer(k):
     assert len(partition.partition_frontier(g, k)) < 0.9 * len(partition.partition_dfs(g, k))
     with pytest.raises(ValueError):
         partition.partition_frontier([Gate("X", (0,), (1, 2))], 2)
+
+
+def test_frames_handles_without_device():
+    """The deferred-factor handle is host-only: created, queried, destroyed;
+    bad sizes are rejected."""
+    fr = abi.Frames(12)
+    assert not fr.pending
+    fr.close()
+    h = ctypes.c_void_p()
+    assert abi.lib().hs_frames_create(0, ctypes.byref(h)) == abi.HS_E_INVALID
+    assert abi.lib().hs_frames_create(64, ctypes.byref(h)) == abi.HS_E_INVALID
+    assert abi.lib().hs_frames_pending(None, None) == abi.HS_E_INVALID
+    assert abi.lib().hs_part_run_carry(None, None, None, 0, None) == abi.HS_E_INVALID
