@@ -168,6 +168,11 @@ struct PartProgram {
   DevOp ops[kMaxOps];            // per group: rotations and others in program order
   uint8_t others[kMaxOps];       // per round: indices into ops of its non-rotation ops
   RoundDesc rounds[kMaxRounds];
+  // per round: up to four sign flips applied right after its rotations,
+  // 16 bits each from bit 0 (0 = none): bits 0-3 register mask M (the
+  // elements whose register bits cover M), bits 4-5 condition (0 none, 1 a
+  // thread tile bit, 2 an outer slot), bits 6-11 its position
+  uint64_t signs[kMaxRounds];
   double2 coef[kMaxCoef];
 };
 static_assert(sizeof(PartProgram) <= 32000, "kernel parameter space");

@@ -449,6 +449,11 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
   uint64_t tile = blockIdx.x;
   // global offset of the tile being processed (computed when its copy is issued)
   uint64_t gbase = tile < P.ntiles ? deposit(tile, P.outer) : 0;
+  // the next tile's offset by an addition in the scattered outer bits: with
+  // every other bit set the carries run through the gaps, so
+  // deposit(t + G) = ((deposit(t) | ~mask) + deposit(G)) & mask
+  const uint64_t omask = deposit(P.ntiles - 1, P.outer);
+  const uint64_t ostep = deposit(uint64_t(gridDim.x), P.outer);
   if (tile < P.ntiles) issue_tile_load<V>(sv, sb0, gbase, s_gchunk, s_cswz, tswz, gt, per_thr, size, tile_bytes);
   cp_async_commit();
   cp_async_wait<0>();
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
   V v[E];
   for (; tile < P.ntiles; tile += gridDim.x) {
     const uint64_t next = tile + gridDim.x;
-    const uint64_t gnext = next < P.ntiles ? deposit(next, P.outer) : 0;
+    const uint64_t gnext = next < P.ntiles ? (((gbase | ~omask) + ostep) & omask) : 0;
     for (int g = 0; g < P.ngroups; ++g) {
       const GroupDesc& G = P.groups[g];
       const bool last = g == P.ngroups - 1;
@@ -506,6 +511,27 @@ __global__ void __launch_bounds__(K1Threads<V, R, FULL, FAST, WIDE>::value, K1Th
   }
         SLOT(0) SLOT(1) SLOT(2) SLOT(3)
 #undef SLOT
+        // the round's sign flips: register mask and at most one condition bit
+        if (const uint64_t sgw = P.signs[r]) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t f = uint32_t(sgw >> (16 * q)) & 0xffffu;
+            if (f == 0u) break;  // entries are packed from the low end
+            const uint32_t kind = (f >> 4) & 3u, pos = (f >> 6) & 63u;
+            const uint32_t bit = kind == 1u   ? (thr >> pos) & 1u
+                                 : kind == 2u ? uint32_t(gbase >> pos) & 1u
+                                              : 1u;
+            const uint32_t sm = bit ? 0x80000000u : 0u;
+#define SNEG(M) \
+  case (M): if constexpr ((M) < (1 << R)) dneg<R, M>(v, sm); break;
+            switch (f & 15u) {
+              SNEG(1) SNEG(2) SNEG(3) SNEG(4) SNEG(5) SNEG(6) SNEG(7)
+              SNEG(8) SNEG(9) SNEG(10) SNEG(11) SNEG(12) SNEG(13) SNEG(14) SNEG(15)
+              default: break;
+            }
+#undef SNEG
+          }
+        }
         const int k0 = int(rw >> 12) & 255, k1 = k0 + (int(rw >> 4) & 255);
         for (int k = k0; k < k1; ++k) {
           run_op<R, FULL, FAST>(v, P.ops[P.others[k]], s_coef, thr, gbase, dfr, P);

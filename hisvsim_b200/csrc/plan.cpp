@@ -527,6 +527,24 @@ bool touches_reg(const DevOp& x, int j) {
 
 bool diagonal_op(const DevOp& x) { return x.kind >= OPD_PHASE; }
 
+// the sign word entry of a sign flip on register elements (mask creg) whose
+// thread / outer condition is at most one bit
+bool sign_entry(const DevOp& x, uint32_t* entry) {
+  if (x.kind != OPD_NEG || x.creg == 0 || x.creg > 15) return false;
+  const int nthr = __builtin_popcount(x.cthr), nout = __builtin_popcountll(x.couter);
+  if (nthr + nout > 1) return false;
+  uint32_t kind = 0, pos = 0;
+  if (nthr) {
+    kind = 1;
+    pos = uint32_t(__builtin_ctz(x.cthr));
+  } else if (nout) {
+    kind = 2;
+    pos = uint32_t(__builtin_ctzll(x.couter));
+  }
+  *entry = uint32_t(x.creg) | kind << 4 | pos << 6;
+  return true;
+}
+
 // Pack the group's ops into rounds (RoundDesc) by list scheduling: op b must
 // follow an earlier op a only when both act on a common register bit and not
 // both are diagonal (ops act non-diagonally on register bits alone, so
@@ -573,17 +591,31 @@ void build_rounds(PartProgram* P, GroupDesc* gd) {
       state[b] = 2;
       --left;
     }
+    // sign flips on register elements with at most one thread / outer
+    // condition go to the round's sign word (applied before its other ops:
+    // valid while every other op placed before them is diagonal)
+    uint64_t signs = 0;
+    int nsign = 0;
+    bool others_diag = true;
     for (bool grew = true; grew;) {
       grew = false;
       for (int b = 0; b < n; ++b) {
-        if (state[b] || P->ops[o0 + b].kind == OP1_ROT || !ready(b, 2)) continue;
-        P->others[P->nothers++] = uint8_t(o0 + b);
-        ++num_other;
+        const DevOp& x = P->ops[o0 + b];
+        if (state[b] || x.kind == OP1_ROT || !ready(b, 2)) continue;
+        uint32_t entry = 0;
+        if (others_diag && nsign < 4 && sign_entry(x, &entry)) {
+          signs |= uint64_t(entry) << (16 * nsign++);
+        } else {
+          P->others[P->nothers++] = uint8_t(o0 + b);
+          ++num_other;
+          if (!diagonal_op(x)) others_diag = false;
+        }
         state[b] = 2;
         --left;
         grew = true;
       }
     }
+    P->signs[P->nrounds] = signs;
     P->rounds[P->nrounds++] = round_pack(zmask, first_other, num_other, pair, form);
     for (int b = 0; b < n; ++b)
       if (state[b] == 2) state[b] = 1;

@@ -265,6 +265,18 @@ void run_program(const PartProgram& P, int ab, std::vector<C>& sv) {
             if (ci + 2 > uint32_t(P.ncoef)) throw std::runtime_error("rotation coefficients out of range");
             run_op(v, R, P, rop, P.coef + ci, thr, gbase, dsign, ab);
           }
+          // the round's sign word: register mask M, at most one condition bit
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t f = uint32_t(P.signs[r] >> (16 * q)) & 0xffffu;
+            if (!f) break;
+            const uint32_t kind = (f >> 4) & 3u, pos = (f >> 6) & 63u;
+            const uint32_t bit = kind == 1u ? (thr >> pos) & 1u
+                                 : kind == 2u ? uint32_t(gbase >> pos) & 1u : 1u;
+            const int M = int(f & 15u);
+            if (bit)
+              for (int e = 0; e < E; ++e)
+                if ((e & M) == M) v[e] = -v[e];
+          }
           const int k0 = int(rw >> 12) & 255, k1 = k0 + (int(rw >> 4) & 255);
           for (int k = k0; k < k1; ++k) {
             const DevOp& op = P.ops[P.others[k]];
