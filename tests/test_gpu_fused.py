@@ -2,8 +2,8 @@
 states on the tensor cores with split-BF16 operands (K4).
 
 Tolerances: composed unitaries match the oracle to 1e-12; the complex64
-result keeps fidelity loss 1 - |<psi_fp64|psi>|^2 <= 1e-6
-and max amplitude error <= 1e-5 against complex128."""
+result keeps fidelity loss 1 - |<psi_fp64|psi>|^2 <= 1e-6 (the precision
+form's bound) and max amplitude error <= 1e-5 against complex128."""
 import numpy as np
 import pytest
 

@@ -1,6 +1,6 @@
 """Learned form on the GPU: the K7 network kernels against the numpy oracle
 (oracle/mlp.py), the timing harvest, and the proposer against the acyclic
-partitioner it falls back to, judged by measured device time.
+partitioner it falls back to, compared by measured device time.
 
 Tolerances: FP32 kernels against the float64 oracle, forward 1e-4 relative,
 gradients 1e-4 of the largest gradient component."""
@@ -95,7 +95,7 @@ def test_harvest_features_and_targets():
 
 
 def test_learned_proposal_beats_acyclic_partitioner():
-    """The method with the network against the method without it, judged by
+    """The method with the network against the method without it, compared by
     measured device time: a 27-qubit complex64 random circuit (40 layers of
     U3 + CZ), the proposal against the acyclic partitioner at its default
     part size (9, the fallback) and at the best size the network finds."""
