@@ -652,13 +652,14 @@ def simulate(program: Program, parts: Optional[Sequence[Sequence[int]]] = None, 
              max_qubits: int = 10, state=None):
     """Run the program's gates on the GPU from |0...0> (or on ``state``) in
     ``parts`` (gate index lists into ``program.circuit()``; default: the
-    acyclic partitioner with ``max_qubits``).  Returns the ``abi.State``."""
+    frontier partitioner with ``max_qubits``, the fewest parts).  Returns the
+    ``abi.State``."""
     from . import abi, partition
     from .gates import part_offsets
 
     gates = program.circuit()
     if parts is None:
-        parts = partition.partition_acyclic(gates, max_qubits) if gates else []
+        parts = partition.partition_frontier(gates, max_qubits) if gates else []
     if state is None:
         state = abi.State(program.num_qubits, dtype)
         state.set_basis(0)
