@@ -278,3 +278,17 @@ def test_frames_handles_without_device():
     assert abi.lib().hs_frames_create(64, ctypes.byref(h)) == abi.HS_E_INVALID
     assert abi.lib().hs_frames_pending(None, None) == abi.HS_E_INVALID
     assert abi.lib().hs_part_run_carry(None, None, None, 0, None) == abi.HS_E_INVALID
+
+
+def test_proposer_segmentation_margin():
+    """A dynamic-programming segmentation replaces the best whole-partition
+    candidate only when predicted faster by more than the margin: with the
+    margin at 1 it never does, with 0 the cheapest prediction wins."""
+    from hisvsim_b200 import learned
+
+    gates = circuits.random_u3_cz(14, 6, 9)
+    strict = learned.propose(gates, 14, _PassCountModel(), ks=(5, 7, 9), dp_margin=1.0)
+    assert not strict["method"].startswith("dp over")
+    loose = learned.propose(gates, 14, _PassCountModel(), ks=(5, 7, 9), dp_margin=0.0)
+    assert loose["predicted_ms"] == pytest.approx(min(loose["candidates"].values()))
+    assert strict["predicted_ms"] >= loose["predicted_ms"]
