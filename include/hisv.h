@@ -157,7 +157,9 @@ int hs_gate_apply(hs_state* st, const hs_gate* gate, void* stream);
 /* gather_and_execute_on (execute.hpp:171; live semantics of
  * gather_and_execute_on_multi, execute.hpp:318-470): one part — every gate of
  * `gates` applied in order inside one K1 launch that stages each 2^m tile of
- * the state on chip and writes it back once. */
+ * the state on chip and writes it back once.  The stored amplitudes are exact
+ * after the call; hs_part_run_carry (below) is the same with the rotations'
+ * pending factors kept for the next part. */
 int hs_part_run(hs_state* st, const hs_gate* gates, int num_gates, void* stream);
 
 /* Several parts back to back (the loop of execute_qasm_parts,
