@@ -29,7 +29,7 @@ from __future__ import annotations
 from collections import OrderedDict
 from typing import Dict, List, Sequence
 
-from .gates import Gate
+from .gates import DIAGONAL, Gate
 
 
 def _check(max_qubits: int, gates: Sequence[Gate]):
@@ -203,8 +203,8 @@ def _absorbable(qset, ready, indeg, succ, qubits) -> int:
     return count
 
 
-def partition_frontier(gates: Sequence[Gate], max_qubits: int,
-                       age_weight: float = 1.0) -> List[List[int]]:
+def partition_frontier(gates: Sequence[Gate], max_qubits: int, age_weight: float = 1.0,
+                       free_diagonal: bool = False) -> List[List[int]]:
     """Acyclic parts grown from the ready frontier of the gate DAG.
 
     A part starts with an empty qubit set S and repeats: absorb every ready
@@ -214,11 +214,20 @@ def partition_frontier(gates: Sequence[Gate], max_qubits: int,
     (``_absorbable``), preferring earlier gates (``age_weight`` * index / N)
     and then fewer new qubits.  The part closes when no ready gate fits.
     Gates are taken only when ready, so the parts in order are a topological
-    order of the DAG."""
+    order of the DAG.
+
+    With ``free_diagonal`` the limit counts only the targets of non-diagonal
+    gates: the part kernel holds those in its tile, while diagonal gates and
+    controls act on index bits wherever they are, so CZ partners and controls
+    cost nothing (for the plain form's K1; a fused unitary needs every qubit
+    its gates touch)."""
     _check(max_qubits, gates)
     n = len(gates)
     succ = dag_successors(gates)
-    qubits = [frozenset(g.qubits) for g in gates]
+    if free_diagonal:
+        qubits = [frozenset() if g.name in DIAGONAL else frozenset(g.targets) for g in gates]
+    else:
+        qubits = [frozenset(g.qubits) for g in gates]
     indeg = [0] * n
     for s in succ:
         for j in s:

@@ -175,3 +175,21 @@ def test_targets_filling_the_tile_leave_out_low_slots(emu, port):
     got64, st64 = emu(n, rec, offs, dtype=1)
     assert st64["passes"] == 2
     assert np.abs(got64 - want).max() <= 1e-5
+
+
+@pytest.mark.parametrize("kind,n,k", [("u3cz", 16, 7), ("u3cz", 17, 9), ("layered", 14, 5),
+                                      ("qft", 13, 6)])
+def test_parts_with_free_diagonal_gates(emu, port, kind, n, k):
+    """Frontier parts whose qubit limit counts only non-diagonal targets (CZ
+    partners and controls act on index bits anywhere): fewer parts, one pass
+    each, the oracle's amplitudes."""
+    gates = _circuit(kind, n, 5)
+    parts = partition.partition_frontier(gates, k, free_diagonal=True)
+    assert partition.is_valid_partition(gates, parts)
+    assert len(parts) < len(partition.partition_frontier(gates, k))
+    rec, offs = part_offsets(partition.parts_to_gates(gates, parts))
+    want = port.run(n, to_records(gates))
+    for per_part in (False, True):
+        got, st = emu(n, rec, offs, per_part=per_part)
+        assert st["passes"] == len(parts)
+        assert np.abs(got - want).max() <= 1e-12
