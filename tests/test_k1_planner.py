@@ -193,3 +193,25 @@ def test_parts_with_free_diagonal_gates(emu, port, kind, n, k):
         got, st = emu(n, rec, offs, per_part=per_part)
         assert st["passes"] == len(parts)
         assert np.abs(got - want).max() <= 1e-12
+
+
+def test_long_part_splits_into_programs(emu, port):
+    """A part with more ops than one program holds (7 rotated qubits, 170
+    controlled phases and sign flips on 12 qubits: one free-diagonal part)
+    runs as two passes with the frames carried between them."""
+    rng = np.random.default_rng(3)
+    n = 12
+    g = [Gate("U3", (q,), params=tuple(rng.uniform(0, 2 * np.pi, 3))) for q in range(7)]
+    for i in range(170):
+        a, b = (int(x) for x in rng.choice(n, 2, replace=False))
+        g.append(Gate("U1", (a,), (b,), params=(float(rng.uniform(0, 2 * np.pi)),)) if i % 2
+                 else Gate("Z", (a,), (b,)))
+    g += [Gate("U3", (q,), params=tuple(rng.uniform(0, 2 * np.pi, 3))) for q in range(7)]
+    parts = partition.partition_frontier(g, 7, free_diagonal=True)
+    assert len(parts) == 1
+    rec, offs = part_offsets(partition.parts_to_gates(g, parts))
+    want = port.run(n, to_records(g))
+    for per_part in (False, True):
+        got, st = emu(n, rec, offs, per_part=per_part)
+        assert st["passes"] == 2
+        assert np.abs(got - want).max() <= 1e-12
