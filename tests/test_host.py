@@ -292,3 +292,25 @@ def test_proposer_segmentation_margin():
     loose = learned.propose(gates, 14, _PassCountModel(), ks=(5, 7, 9), dp_margin=0.0)
     assert loose["predicted_ms"] == pytest.approx(min(loose["candidates"].values()))
     assert strict["predicted_ms"] >= loose["predicted_ms"]
+
+
+def test_bench_partitions(monkeypatch):
+    """The benchmark's part choices: the plain form's frontier parts bound only
+    non-diagonal targets, the precision form's and the reference path's every
+    touched qubit; all are valid partitions of the workload."""
+    import sys
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    args = bench.parse()
+    gates, parts, rec, offs = bench.workload(20, 6, 1, 9, bench.plain_partitioner(args))
+    assert partition.is_valid_partition(gates, parts) and int(offs[-1]) == len(gates)
+    bounded = bench.partitioner(args)(gates, 9)
+    assert partition.is_valid_partition(gates, bounded)
+    assert len(parts) < len(bounded)
+    for p in bounded:
+        assert len({q for i in p for q in gates[i].qubits}) <= 9
+    fused = bench.partitioner(args)(gates, 6)
+    assert all(len({q for i in p for q in gates[i].qubits}) <= 6 for p in fused)
